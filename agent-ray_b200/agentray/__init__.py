@@ -1,0 +1,259 @@
+"""agentray — Python host mirror of agent-ray's rendering API over libagentray.
+
+The reference crate's surface (src/integrators/mod.rs:18-26, src/scene.rs,
+src/cameras.rs, src/film.rs) maps as follows:
+
+  Scene::new(objects, lights, light_dist)      -> Scene(context, scene_data)
+  PinholeCamera::from_lookat(...)              -> Camera(lookfrom, lookat, vup, vfov, aspect)
+  PathTracer::new(PathTracerConfig{..})        -> PathTracer(PathTracerConfig(..))
+  BidirectionalPathTracer / BdptConfig         -> BidirectionalPathTracer(BdptConfig(..))
+  GradientDomainPathTracer / GdptConfig        -> GradientDomainPathTracer(GdptConfig(..))
+  Integrator::render(&scene, &camera, w, h)    -> integrator.render(scene, camera, w, h) -> Film
+  Film::to_hdr_vec()                           -> Film.to_hdr_vec()  ((H*W, 3) float32)
+  Scene::intersect / occluded (ray batches)    -> Scene.trace_closest / Scene.trace_any
+
+All work runs in the CUDA library; nothing here computes on the CPU.
+"""
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _abi as A
+from ._lib import AgentRayError, check, lib
+from .scene_data import Camera, Light, Material, Mesh, Object, SceneData, integrator_cfg
+
+__all__ = ["Context", "Scene", "Camera", "Film", "PathTracer", "PathTracerConfig", "BidirectionalPathTracer",
+           "BdptConfig", "GradientDomainPathTracer", "GdptConfig", "SceneData", "Mesh", "Object", "Material",
+           "Light", "AgentRayError", "integrator_cfg", "lib"]
+
+
+class Context:
+    """One CUDA device + stream (ar_context)."""
+
+    def __init__(self, device=0):
+        self.handle = C.c_void_p()
+        check(lib().ar_context_create(device, C.byref(self.handle)))
+
+    def set_stream(self, stream_ptr):
+        check(lib().ar_context_set_stream(self.handle, C.c_void_p(stream_ptr)))
+
+    def synchronize(self):
+        check(lib().ar_context_synchronize(self.handle))
+
+    def render_stats(self):
+        s = A.RenderStats()
+        check(lib().ar_get_render_stats(self.handle, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in A.RenderStats._fields_}
+
+    def profile(self, enable=True):
+        check(lib().ar_profile_enable(self.handle, 1 if enable else 0))
+
+    def profile_reset(self):
+        check(lib().ar_profile_reset(self.handle))
+
+    def profile_read(self):
+        """{kernel name: (launches, summed device ms)} since the last reset."""
+        cap = 64
+        names = C.create_string_buffer(8192)
+        ms = (C.c_double * cap)()
+        ln = (C.c_uint64 * cap)()
+        n = C.c_uint32(cap)
+        check(lib().ar_profile_read(self.handle, names, 8192, ms, ln, C.byref(n)))
+        keys = names.value.decode().split("\n")[: n.value]
+        return {k: (int(ln[i]), float(ms[i])) for i, k in enumerate(keys)}
+
+    def close(self):
+        if self.handle:
+            lib().ar_context_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Scene:
+    """Device-resident scene with its acceleration structures (Scene::new)."""
+
+    def __init__(self, ctx: Context, data: SceneData):
+        self.ctx = ctx
+        self.data = data
+        self.handle = C.c_void_p()
+        desc, keep = data.desc()
+        check(lib().ar_scene_create(ctx.handle, C.byref(desc), C.byref(self.handle)))
+        del keep
+
+    def stats(self):
+        s = A.SceneStats()
+        check(lib().ar_scene_get_stats(self.handle, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in A.SceneStats._fields_ if not k.startswith("_")}
+
+    def rebuild(self, max_leaf_size=3, sah_bins=32, build_threads=0):
+        o = A.AccelOpts(max_leaf_size, sah_bins, build_threads, 0)
+        check(lib().ar_scene_build_accel(self.ctx.handle, self.handle, C.byref(o)))
+
+    @staticmethod
+    def _batch(org_tmin, dir_tmax, on_device):
+        b = A.RayBatch()
+        if on_device:
+            b.org_tmin, b.dir_tmax, b.count = org_tmin.data_ptr(), dir_tmax.data_ptr(), org_tmin.shape[0]
+        else:
+            b.org_tmin, b.dir_tmax, b.count = org_tmin.ctypes.data, dir_tmax.ctypes.data, org_tmin.shape[0]
+        b.on_device = 1 if on_device else 0
+        return b
+
+    def trace_closest(self, org_tmin, dir_tmax):
+        """Closest hit for (n,4) float32 ray arrays (numpy on the host, or torch
+        CUDA tensors).  Returns (hits (n,4): t,u,v,prim_id-bits; inst_ids (n,))."""
+        dev = not isinstance(org_tmin, np.ndarray)
+        if dev:
+            import torch
+            hits = torch.empty((org_tmin.shape[0], 4), dtype=torch.float32, device=org_tmin.device)
+            inst = torch.empty((org_tmin.shape[0],), dtype=torch.int32, device=org_tmin.device)
+            b = self._batch(org_tmin, dir_tmax, True)
+            check(lib().ar_trace_closest(self.ctx.handle, self.handle, C.byref(b), hits.data_ptr(),
+                                         inst.data_ptr(), 1))
+            return hits, inst
+        org_tmin = np.ascontiguousarray(org_tmin, np.float32)
+        dir_tmax = np.ascontiguousarray(dir_tmax, np.float32)
+        n = org_tmin.shape[0]
+        hits = np.empty((n, 4), np.float32)
+        inst = np.empty(n, np.uint32)
+        b = self._batch(org_tmin, dir_tmax, False)
+        check(lib().ar_trace_closest(self.ctx.handle, self.handle, C.byref(b), hits.ctypes.data, inst.ctypes.data,
+                                     0))
+        return hits, inst
+
+    def trace_any(self, org_tmin, dir_tmax):
+        org_tmin = np.ascontiguousarray(org_tmin, np.float32)
+        dir_tmax = np.ascontiguousarray(dir_tmax, np.float32)
+        occ = np.empty(org_tmin.shape[0], np.uint8)
+        b = self._batch(org_tmin, dir_tmax, False)
+        check(lib().ar_trace_any(self.ctx.handle, self.handle, C.byref(b), occ.ctypes.data, 0))
+        return occ
+
+    def close(self):
+        if self.handle:
+            lib().ar_scene_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Film:
+    """Linear HDR film (src/film.rs), already divided by spp."""
+
+    def __init__(self, rgb: np.ndarray, width: int, height: int):
+        self.rgb = rgb.reshape(height, width, 3)
+        self.width = width
+        self.height = height
+
+    def to_hdr_vec(self):
+        return self.rgb.reshape(-1, 3)
+
+    def get_pixel(self, x, y):
+        return self.rgb[y, x]
+
+
+@dataclass
+class PathTracerConfig:
+    """src/integrators/path_tracer.rs:18-31"""
+    spp: int = 64
+    max_depth: int = 8
+    rr_depth: int = 3
+    seed: int = 0
+    film_precision: int = A.FILM_F32
+
+
+@dataclass
+class BdptConfig:
+    """src/integrators/bidirectional_path_tracer.rs:102-133"""
+    spp: int = 64
+    max_depth: int = 8
+    rr_depth: int = 3
+    mis_mode: int = A.MIS_POWER
+    mis_beta: float = 2.0
+    seed: int = 0
+    film_precision: int = A.FILM_F32
+
+
+@dataclass
+class GdptConfig:
+    """src/integrators/gradient_domain_pt.rs:47-76 (+ solver choice)."""
+    spp: int = 64
+    max_depth: int = 8
+    rr_depth: int = 3
+    alpha: float = 0.2
+    poisson_iterations: int = 200
+    sor_omega: float = 1.6
+    poisson_solver: int = A.POISSON_SOR
+    poisson_tolerance: float = 1e-6
+    seed: int = 0
+    film_precision: int = A.FILM_F32
+
+
+class _Integrator:
+    kind = A.INTEGRATOR_PT
+
+    def __init__(self, config):
+        self.config = config
+
+    def cfg(self):
+        c = self.config
+        return integrator_cfg(self.kind, spp=c.spp, max_depth=c.max_depth, rr_depth=c.rr_depth,
+                              mis_mode=getattr(c, "mis_mode", A.MIS_POWER), mis_beta=getattr(c, "mis_beta", 2.0),
+                              alpha=getattr(c, "alpha", 0.2), poisson_iterations=getattr(c, "poisson_iterations", 200),
+                              sor_omega=getattr(c, "sor_omega", 1.6),
+                              poisson_solver=getattr(c, "poisson_solver", A.POISSON_SOR),
+                              poisson_tolerance=getattr(c, "poisson_tolerance", 1e-6), seed=c.seed,
+                              film_precision=c.film_precision)
+
+    def render(self, scene: Scene, camera: Camera, width: int, height: int, out=None) -> Film:
+        """Integrator::render.  `out` may be a CUDA float32 tensor of W*H*3 to
+        keep the image on the device."""
+        cfg = self.cfg()
+        cam = camera.desc()
+        if out is not None and not isinstance(out, np.ndarray):
+            check(lib().ar_render(scene.ctx.handle, scene.handle, C.byref(cam), C.byref(cfg), width, height,
+                                  out.data_ptr(), 1))
+            return out
+        buf = np.empty(width * height * 3, np.float32) if out is None else out
+        check(lib().ar_render(scene.ctx.handle, scene.handle, C.byref(cam), C.byref(cfg), width, height,
+                              buf.ctypes.data, 0))
+        return Film(buf, width, height)
+
+
+class PathTracer(_Integrator):
+    kind = A.INTEGRATOR_PT
+
+
+class BidirectionalPathTracer(_Integrator):
+    kind = A.INTEGRATOR_BDPT
+
+
+class GradientDomainPathTracer(_Integrator):
+    kind = A.INTEGRATOR_GDPT
+
+
+def poisson_reconstruct(ctx: Context, primal, grad_x, grad_y, alpha=0.2, solver=A.POISSON_SOR, iterations=200,
+                        omega=1.6, tolerance=1e-6):
+    """screened_poisson_reconstruct on the GPU for (H, W, 3) float32 films.
+    Returns (image, fp64 relative residual or -1 for SOR)."""
+    h, w, _ = primal.shape
+    p = np.ascontiguousarray(primal, np.float32)
+    x = np.ascontiguousarray(grad_x, np.float32)
+    y = np.ascontiguousarray(grad_y, np.float32)
+    out = np.empty_like(p)
+    cfg = integrator_cfg(A.INTEGRATOR_GDPT, alpha=alpha, poisson_iterations=iterations, sor_omega=omega,
+                         poisson_solver=solver, poisson_tolerance=tolerance)
+    res = C.c_double(0.0)
+    check(lib().ar_poisson_reconstruct(ctx.handle, C.byref(cfg), w, h, p.ctypes.data, x.ctypes.data, y.ctypes.data,
+                                       out.ctypes.data, 0, C.byref(res)))
+    return out, res.value

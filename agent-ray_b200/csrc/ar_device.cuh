@@ -1,0 +1,341 @@
+// Device-side math, sampler and BVH8 traversal for the light-transport kernels.
+//
+// Parity-critical arithmetic (ray normalisation, instance transforms and the
+// Möller–Trumbore test) uses explicitly rounded intrinsics so that no multiply
+// is fused into an add: the reference (Rust + glam SSE2) computes these with
+// separate roundings, and the closest-hit t/u/v must match it bit for bit.
+#pragma once
+#include <cfloat>
+#include <cstdint>
+#include "ar_types.h"
+
+namespace ar {
+
+struct f3 {
+    float x, y, z;
+};
+__device__ __forceinline__ f3 mk(float x, float y, float z) { return {x, y, z}; }
+__device__ __forceinline__ f3 operator+(f3 a, f3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ f3 operator-(f3 a, f3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ f3 operator-(f3 a) { return {-a.x, -a.y, -a.z}; }
+__device__ __forceinline__ f3 operator*(f3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ f3 operator*(float s, f3 a) { return {a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ f3 operator*(f3 a, f3 b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
+__device__ __forceinline__ f3 operator/(f3 a, float s) { return {a.x / s, a.y / s, a.z / s}; }
+__device__ __forceinline__ float dot(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ f3 cross(f3 a, f3 b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ float length(f3 a) { return sqrtf(dot(a, a)); }
+__device__ __forceinline__ f3 normalize(f3 a) { return a * (1.0f / length(a)); }
+__device__ __forceinline__ float max3(f3 a) { return fmaxf(fmaxf(a.x, a.y), a.z); }
+__device__ __forceinline__ bool is_zero(f3 a) { return a.x == 0.f && a.y == 0.f && a.z == 0.f; }
+
+// ---- exactly rounded (no contraction) variants: reference arithmetic order ----
+__device__ __forceinline__ f3 sub_rn(f3 a, f3 b) {
+    return {__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z)};
+}
+__device__ __forceinline__ f3 add_rn(f3 a, f3 b) {
+    return {__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z)};
+}
+__device__ __forceinline__ f3 scale_rn(f3 a, float s) {
+    return {__fmul_rn(a.x, s), __fmul_rn(a.y, s), __fmul_rn(a.z, s)};
+}
+// glam dot3: (x*x' + y*y') + z*z'
+__device__ __forceinline__ float dot_rn(f3 a, f3 b) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
+__device__ __forceinline__ f3 cross_rn(f3 a, f3 b) {
+    return {__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)), __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(a.x, b.z)),
+            __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x))};
+}
+// glam normalize: v * (1 / sqrt(dot(v, v)))
+__device__ __forceinline__ f3 normalize_rn(f3 a) {
+    return scale_rn(a, __fdiv_rn(1.0f, __fsqrt_rn(dot_rn(a, a))));
+}
+__device__ __forceinline__ f3 ld3(const float* p) { return {p[0], p[1], p[2]}; }
+
+// ---- counter-based sampler (SplitMix64 finalizer, Steele et al. 2014) ----
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+__device__ __forceinline__ uint64_t counter_key(uint64_t seed, uint32_t pixel, uint32_t sample) {
+    return mix64(seed ^ mix64((uint64_t(pixel) << 32) | uint64_t(sample)));
+}
+__device__ __forceinline__ float counter_u01(uint64_t key, uint32_t dim) {
+    uint64_t z = mix64(key + uint64_t(dim + 1) * 0x9e3779b97f4a7c15ull);
+    return float(uint32_t(z >> 40)) * (1.0f / 16777216.0f);
+}
+constexpr uint32_t kLightSubpathDim = 4096;
+
+// ---- traversal ----
+struct Ray {
+    f3 o, d;
+    float tmin, tmax;
+};
+
+struct HitRec {
+    float t, u, v;
+    uint32_t slot;  // triangle record index (leaf order), kInvalid on miss
+    uint32_t inst;  // SceneObject index
+};
+
+// Ray::new applied to a world ray (direction normalised as glam does).
+__device__ __forceinline__ Ray make_ray(f3 o, f3 d, float tmin, float tmax) { return {o, normalize_rn(d), tmin, tmax}; }
+
+// Triangle::hit (src/geometry.rs:172-206) with the reference's operation order.
+__device__ __forceinline__ bool tri_test(const TriRecord& tr, f3 o, f3 d, float tmin, float tmax, float& t, float& u,
+                                         float& v) {
+    f3 v0 = mk(tr.v0x, tr.v0y, tr.v0z), e1 = mk(tr.e1x, tr.e1y, tr.e1z), e2 = mk(tr.e2x, tr.e2y, tr.e2z);
+    f3 h = cross_rn(d, e2);
+    float a = dot_rn(e1, h);
+    if (fabsf(a) < 1e-8f) return false;
+    float f = __fdiv_rn(1.0f, a);
+    f3 s = sub_rn(o, v0);
+    float uu = __fmul_rn(f, dot_rn(s, h));
+    if (uu < 0.0f || uu > 1.0f) return false;
+    f3 q = cross_rn(s, e1);
+    float vv = __fmul_rn(f, dot_rn(d, q));
+    if (vv < 0.0f || __fadd_rn(uu, vv) > 1.0f) return false;
+    float tt = __fmul_rn(f, dot_rn(e2, q));
+    if (tt < tmin || tt > tmax) return false;
+    t = tt;
+    u = uu;
+    v = vv;
+    return true;
+}
+
+__device__ __forceinline__ TriRecord load_tri(const TriRecord* tris, uint32_t i) {
+    const float4* p = reinterpret_cast<const float4*>(tris + i);
+    float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
+    TriRecord r;
+    r.v0x = a.x; r.v0y = a.y; r.v0z = a.z; r.prim = __float_as_uint(a.w);
+    r.e1x = b.x; r.e1y = b.y; r.e1z = b.z; r.object_local = __float_as_uint(b.w);
+    r.e2x = c.x; r.e2y = c.y; r.e2z = c.z; r.pad = __float_as_uint(c.w);
+    return r;
+}
+
+// Per-ray constants of the slab test.
+struct RayPre {
+    f3 o, inv;
+    uint32_t oct;  // bit k set when direction k is negative
+    float tmin;
+};
+__device__ __forceinline__ RayPre precompute(f3 o, f3 d, float tmin) {
+    RayPre r;
+    r.o = o;
+    const float eps = 1e-20f;
+    r.inv.x = 1.0f / (fabsf(d.x) > eps ? d.x : copysignf(eps, d.x));
+    r.inv.y = 1.0f / (fabsf(d.y) > eps ? d.y : copysignf(eps, d.y));
+    r.inv.z = 1.0f / (fabsf(d.z) > eps ? d.z : copysignf(eps, d.z));
+    r.oct = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
+    r.tmin = tmin;
+    return r;
+}
+
+__device__ __forceinline__ uint32_t byte_of(uint32_t w, uint32_t i) { return (w >> (8 * i)) & 0xffu; }
+
+// Intersects the 8 children of node `ni`.  Outputs the node group (bits 8..15:
+// internal-child hits in traversal order i, bits 0..7: imask) and the leaf
+// primitive hit mask relative to tri_base.
+__device__ __forceinline__ void intersect_node(const WideNode* nodes, uint32_t ni, const RayPre& r, float tmax,
+                                               uint32_t& child_base, uint32_t& node_bits, uint32_t& tri_base,
+                                               uint32_t& tri_bits) {
+    const uint4* np = reinterpret_cast<const uint4*>(nodes + ni);
+    uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
+    const float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
+    const uint32_t ex = w0.w & 0xffu, ey = (w0.w >> 8) & 0xffu, ez = (w0.w >> 16) & 0xffu;
+    const uint32_t imask = w0.w >> 24;
+    const float ax = __uint_as_float(ex << 23) * r.inv.x;
+    const float ay = __uint_as_float(ey << 23) * r.inv.y;
+    const float az = __uint_as_float(ez << 23) * r.inv.z;
+    const float bx = (px - r.o.x) * r.inv.x;
+    const float by = (py - r.o.y) * r.inv.y;
+    const float bz = (pz - r.o.z) * r.inv.z;
+    child_base = w1.x;
+    tri_base = w1.y;
+    // near/far plane bytes per axis, chosen by the ray octant
+    const bool nx = r.oct & 1u, ny = r.oct & 2u, nz = r.oct & 4u;
+    uint32_t nb = 0, tb = 0;
+    const float tfar_limit = tmax * 1.0000004f;
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+        const uint32_t meta = half ? w1.w : w1.z;
+        const uint32_t lox = half ? w2.y : w2.x, loy = half ? w2.w : w2.z, loz = half ? w3.y : w3.x;
+        const uint32_t hix = half ? w3.w : w3.z, hiy = half ? w4.y : w4.x, hiz = half ? w4.w : w4.z;
+        const uint32_t nxw = nx ? hix : lox, fxw = nx ? lox : hix;
+        const uint32_t nyw = ny ? hiy : loy, fyw = ny ? loy : hiy;
+        const uint32_t nzw = nz ? hiz : loz, fzw = nz ? loz : hiz;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const float tnx = fmaf(float(byte_of(nxw, j)), ax, bx);
+            const float tfx = fmaf(float(byte_of(fxw, j)), ax, bx);
+            const float tny = fmaf(float(byte_of(nyw, j)), ay, by);
+            const float tfy = fmaf(float(byte_of(fyw, j)), ay, by);
+            const float tnz = fmaf(float(byte_of(nzw, j)), az, bz);
+            const float tfz = fmaf(float(byte_of(fzw, j)), az, bz);
+            const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, r.tmin));
+            const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tfar_limit));
+            const uint32_t s = uint32_t(half * 4 + j);
+            if (tn <= tf) {
+                const uint32_t m = byte_of(meta, j);
+                if (imask & (1u << s)) {
+                    nb |= 1u << (s ^ r.oct);
+                } else if (m) {
+                    const uint32_t cnt = m >> 5, off = m & 31u;
+                    tb |= ((1u << cnt) - 1u) << off;
+                }
+            }
+        }
+    }
+    node_bits = (nb << 8) | imask;
+    tri_bits = tb;
+}
+
+// Two-level closest-hit / any-hit traversal (TLAS::intersect + BLASAccel::intersect,
+// src/accel/bvh.rs:247-296, :413-447).  One stack serves both levels: entering
+// an instance pushes a marker so that popping it restores the world ray.
+// Returns false (and flags *err) on stack overflow.
+template <bool kAnyHit>
+__device__ bool traverse(const DevScene& sc, const Ray& world, HitRec& hit, int* err) {
+    hit.t = world.tmax;
+    hit.slot = kInvalid;
+    hit.inst = kInvalid;
+    hit.u = hit.v = 0.f;
+    if (sc.tlas_root == kInvalid) return true;
+
+    uint2 stack[kTraversalStack];
+    int sp = 0;
+    const uint32_t kNodeGroup = 0x80000000u, kMarker = 0x40000000u;
+
+    RayPre pre = precompute(world.o, world.d, world.tmin);
+    bool in_blas = false;
+    Ray local;
+    float ds = 1.f;
+    uint32_t cur_inst = kInvalid;
+    float best_l = 0.f, bu = 0.f, bv = 0.f;
+    uint32_t best_l_slot = kInvalid;
+
+    uint2 group = make_uint2(0, 0);  // current node group
+    uint32_t node = sc.tlas_root;
+    bool visit = true;
+    // Bounded loop: a well-formed tree ends far earlier; a corrupt one sets the
+    // error flag instead of spinning.
+    for (uint32_t guard = 0;; ++guard) {
+        if (guard > (1u << 22)) { atomicExch(err, 3); return false; }
+        if (visit) {
+            visit = false;
+            uint32_t cb, nbits, tbase, tbits;
+            intersect_node(sc.nodes, node, pre, in_blas ? best_l : hit.t, cb, nbits, tbase, tbits);
+            group = make_uint2(cb, nbits | kNodeGroup);
+            if (tbits) {
+                if (in_blas) {
+                    while (tbits) {
+                        const uint32_t b = __ffs(tbits) - 1;
+                        tbits &= tbits - 1;
+                        const TriRecord tr = load_tri(sc.tris, tbase + b);
+                        float t, u, v;
+                        if (tri_test(tr, local.o, local.d, local.tmin, best_l, t, u, v) && t < best_l) {
+                            if (kAnyHit) {
+                                if (__fdiv_rn(t, ds) < world.tmax) {
+                                    hit.t = t;
+                                    hit.slot = tbase + b;
+                                    hit.inst = cur_inst;
+                                    return true;
+                                }
+                            } else {
+                                best_l = t;
+                                best_l_slot = tbase + b;
+                                bu = u;
+                                bv = v;
+                            }
+                        }
+                    }
+                } else {
+                    // TLAS leaves: resume the node group after the instances.
+                    if ((group.y >> 8) & 0xffu) {
+                        if (sp >= kTraversalStack) { atomicExch(err, 1); return false; }
+                        stack[sp++] = group;
+                    }
+                    group = make_uint2(0, 0);
+                    if (sp >= kTraversalStack) { atomicExch(err, 1); return false; }
+                    stack[sp++] = make_uint2(tbase, tbits);  // leaf group (instances)
+                }
+            }
+        }
+        // Choose the next node from the current group, else pop.
+        if ((group.y & kNodeGroup) && ((group.y >> 8) & 0xffu)) {
+            const uint32_t hits = (group.y >> 8) & 0xffu;
+            const uint32_t i = __ffs(hits) - 1;
+            const uint32_t s = i ^ pre.oct;
+            const uint32_t imask = group.y & 0xffu;
+            node = group.x + __popc(imask & ((1u << s) - 1u));
+            group.y &= ~(1u << (8 + i));
+            if ((group.y >> 8) & 0xffu) {
+                if (sp >= kTraversalStack) { atomicExch(err, 1); return false; }
+                stack[sp++] = group;
+            }
+            group = make_uint2(0, 0);
+            visit = true;
+            continue;
+        }
+        if (sp == 0) break;
+        uint2 e = stack[--sp];
+        if (e.y & kNodeGroup) {
+            group = e;
+            continue;
+        }
+        if (e.y & kMarker) {
+            // Leave the instance: convert the local best back to world t.
+            if (!kAnyHit && best_l_slot != kInvalid) {
+                const float tw = __fdiv_rn(best_l, ds);
+                if (tw < hit.t) {
+                    hit.t = tw;
+                    hit.slot = best_l_slot;
+                    hit.inst = cur_inst;
+                    hit.u = bu;
+                    hit.v = bv;
+                }
+            }
+            in_blas = false;
+            pre = precompute(world.o, world.d, world.tmin);
+            group = make_uint2(0, 0);
+            continue;
+        }
+        // Instance leaf group: enter the next instance.
+        uint32_t bits = e.y;
+        const uint32_t b = __ffs(bits) - 1;
+        bits &= bits - 1;
+        if (bits) stack[sp++] = make_uint2(e.x, bits);
+        const InstanceRecord* ir = sc.instances + (e.x + b);
+        const float4* ip = reinterpret_cast<const float4*>(ir);
+        const float4 m0 = __ldg(ip), m1 = __ldg(ip + 1), m2 = __ldg(ip + 2);
+        const uint4 m3 = __ldg(reinterpret_cast<const uint4*>(ip + 3));
+        if (!m3.z) continue;  // mesh without triangles
+        const f3 c0 = mk(m0.x, m0.y, m0.z), c1 = mk(m0.w, m1.x, m1.y), c2 = mk(m1.z, m1.w, m2.x),
+                 c3 = mk(m2.y, m2.z, m2.w);
+        // glam transform_point3a / transform_vector3a: ((c0*x + c1*y) + c2*z) + c3
+        const f3 lo = add_rn(c3, add_rn(add_rn(scale_rn(c0, world.o.x), scale_rn(c1, world.o.y)), scale_rn(c2, world.o.z)));
+        const f3 ldu = add_rn(add_rn(scale_rn(c0, world.d.x), scale_rn(c1, world.d.y)), scale_rn(c2, world.d.z));
+        const float scale = __fsqrt_rn(dot_rn(ldu, ldu));
+        if (scale < FLT_EPSILON) continue;
+        ds = scale;
+        local.o = lo;
+        local.d = normalize_rn(ldu);
+        local.tmin = __fmul_rn(world.tmin, ds);
+        best_l = __fmul_rn(kAnyHit ? world.tmax : hit.t, ds);
+        best_l_slot = kInvalid;
+        cur_inst = m3.y;
+        in_blas = true;
+        pre = precompute(local.o, local.d, local.tmin);
+        if (sp >= kTraversalStack) { atomicExch(err, 1); return false; }
+        stack[sp++] = make_uint2(0, kMarker);
+        node = m3.x;
+        visit = true;
+    }
+    return true;
+}
+
+}  // namespace ar

@@ -1,0 +1,269 @@
+// Device shading layer: shading points, BSDFs, lights and the camera.
+// Mirrors the reference operation order; translation units that include this
+// are compiled with -fmad=false so no multiply is fused into an add (the
+// reference Rust/glam code rounds each operation separately).
+//   Scene::intersect shading     src/scene.rs:142-162, :55-87
+//   Onb                          src/geometry.rs:218-244
+//   Lambertian                   src/surfaces/lambertian.rs:35-64
+//   ConductorBsdf (GGX)          src/surfaces/microfacet.rs:14-152
+//   PointLight                   src/lights/point.rs:48-100
+//   Uniform/PowerLightDistribution src/lights.rs:136-235
+//   PinholeCamera                src/cameras.rs:146-248
+// Quad lights are the area-light extension shared with the oracle.
+#pragma once
+#include "ar_device.cuh"
+#include "ar_render.hpp"
+
+namespace ar {
+
+constexpr float kPi = 3.14159265358979323846f;
+constexpr float kInvPi = 0.318309886183790671538f;
+
+struct Onb {
+    f3 n, t, b;
+};
+__device__ __forceinline__ Onb onb_from_normal(f3 nin) {
+    Onb o;
+    o.n = normalize(nin);
+    f3 a = fabsf(o.n.x) > 0.9f ? mk(0.f, 1.f, 0.f) : mk(1.f, 0.f, 0.f);
+    o.b = normalize(cross(o.n, a));
+    o.t = cross(o.b, o.n);
+    return o;
+}
+__device__ __forceinline__ f3 to_local(const Onb& o, f3 v) { return mk(dot(v, o.t), dot(v, o.b), dot(v, o.n)); }
+__device__ __forceinline__ f3 to_world(const Onb& o, f3 v) { return (o.t * v.x + o.b * v.y) + o.n * v.z; }
+__device__ __forceinline__ float signum(float a) { return copysignf(1.0f, a); }
+
+struct Shade {
+    f3 p, n;
+    Onb onb;
+    uint32_t mat;
+    uint32_t prim;
+};
+
+// Scene::intersect post-processing: world shading normal (interpolated vertex
+// normal or geometric normal through the normal matrix), face-forwarded
+// toward the incoming ray, ONB and material.
+__device__ __forceinline__ Shade make_shade(const DevScene& sc, f3 ro, f3 rd, float t, float u, float v, uint32_t slot,
+                                           uint32_t inst) {
+    Shade s;
+    const TriRecord tr = load_tri(sc.tris, slot);
+    const ObjectRecord& ob = sc.objects[inst];
+    const MeshRecord mr = sc.meshes[ob.mesh];
+    s.prim = tr.prim;
+    f3 nobj = normalize(cross(mk(tr.e1x, tr.e1y, tr.e1z), mk(tr.e2x, tr.e2y, tr.e2z)));
+    if (mr.nrm_offset != kInvalid) {
+        const uint32_t* ix = sc.indices + mr.idx_offset + 3 * tr.prim;
+        const float* nb = sc.normals + 3 * size_t(mr.nrm_offset);
+        f3 n0 = ld3(nb + 3 * size_t(ix[0])), n1 = ld3(nb + 3 * size_t(ix[1])), n2 = ld3(nb + 3 * size_t(ix[2]));
+        float w = (1.0f - u) - v;
+        nobj = normalize((n0 * w + n1 * u) + n2 * v);
+    }
+    f3 c0 = mk(ob.nmat[0], ob.nmat[1], ob.nmat[2]), c1 = mk(ob.nmat[3], ob.nmat[4], ob.nmat[5]),
+       c2 = mk(ob.nmat[6], ob.nmat[7], ob.nmat[8]);
+    f3 n = normalize((c0 * nobj.x + c1 * nobj.y) + c2 * nobj.z);
+    f3 wo = -rd;
+    if (dot(n, wo) < 0.f) n = -n;
+    s.n = n;
+    s.onb = onb_from_normal(n);
+    s.p = ro + rd * t;
+    const uint32_t si = mr.num_slots == 1 ? sc.material_slots[mr.slot_offset]
+                                          : sc.material_slots[mr.slot_offset + tr.prim];
+    const uint32_t k = min(si, ob.num_mats - 1);
+    s.mat = sc.material_table[ob.mat_offset + k];
+    return s;
+}
+
+// ---- BSDF (local frame, n = +Z) ----
+__device__ __forceinline__ bool same_hemi(f3 a, f3 b) { return a.z * b.z > 0.f; }
+__device__ __forceinline__ f3 cosine_hemisphere(float ux, float uy) {
+    float r = sqrtf(ux);
+    float phi = (2.0f * kPi) * uy;
+    float x = r * cosf(phi), y = r * sinf(phi);
+    float z = sqrtf(fmaxf((1.0f - x * x) - y * y, 0.0f));
+    return mk(x, y, z);
+}
+__device__ __forceinline__ float ggx_d(float a, f3 h) {
+    float a2 = a * a;
+    float c2 = h.z * h.z;
+    float den = c2 * (a2 - 1.0f) + 1.0f;
+    return a2 / ((kPi * den) * den);
+}
+__device__ __forceinline__ float ggx_lambda(float a, f3 v) {
+    float c2 = v.z * v.z;
+    if (c2 <= 0.f) return INFINITY;
+    float a2 = a * a;
+    float tan2 = (1.0f - c2) / c2;
+    return (sqrtf(1.0f + a2 * tan2) - 1.0f) * 0.5f;
+}
+__device__ __forceinline__ f3 fresnel_schlick(float ci, const float* f0) {
+    float c = fminf(fmaxf(1.0f - fabsf(ci), 0.0f), 1.0f);
+    float c2 = c * c;
+    float t = c * (c2 * c2);
+    return mk(f0[0] + (1.0f - f0[0]) * t, f0[1] + (1.0f - f0[1]) * t, f0[2] + (1.0f - f0[2]) * t);
+}
+
+struct MatView {
+    uint32_t kind;
+    int32_t emitter;
+    float albedo[3], f0[3];
+    float alpha;
+};
+__device__ __forceinline__ MatView load_mat(const DevScene& sc, uint32_t m) {
+    const MaterialRecord& r = sc.materials[m];
+    MatView v;
+    v.kind = r.kind;
+    v.emitter = r.emitter;
+    for (int k = 0; k < 3; ++k) { v.albedo[k] = r.albedo[k]; v.f0[k] = r.f0[k]; }
+    v.alpha = r.alpha;
+    return v;
+}
+
+__device__ __forceinline__ f3 bsdf_eval(const MatView& m, f3 wi, f3 wo) {
+    if (!same_hemi(wi, wo)) return mk(0.f, 0.f, 0.f);
+    if (m.kind == AR_MATERIAL_LAMBERTIAN) return mk(m.albedo[0] * kInvPi, m.albedo[1] * kInvPi, m.albedo[2] * kInvPi);
+    float ci = fabsf(wi.z), co = fabsf(wo.z);
+    if (ci == 0.f || co == 0.f) return mk(0.f, 0.f, 0.f);
+    f3 h = normalize(wi + wo);
+    f3 f = fresnel_schlick(fabsf(dot(wi, h)), m.f0);
+    float d = ggx_d(m.alpha, h);
+    float g = 1.0f / ((1.0f + ggx_lambda(m.alpha, wi)) + ggx_lambda(m.alpha, wo));
+    return f * (d * g / ((4.0f * ci) * co));
+}
+__device__ __forceinline__ float bsdf_pdf(const MatView& m, f3 wi, f3 wo) {
+    if (!same_hemi(wi, wo)) return 0.f;
+    if (m.kind == AR_MATERIAL_LAMBERTIAN) return fabsf(wi.z) * kInvPi;
+    f3 h = normalize(wi + wo);
+    float whwi = fabsf(dot(wi, h));
+    if (whwi == 0.f) return 0.f;
+    return ggx_d(m.alpha, h) * fabsf(h.z) / (4.0f * whwi);
+}
+// Returns false when the reference returns None.
+__device__ __forceinline__ bool bsdf_sample(const MatView& m, f3 wo, float ux, float uy, f3& wi, float& pdf, f3& f) {
+    if (m.kind == AR_MATERIAL_LAMBERTIAN) {
+        wi = cosine_hemisphere(ux, uy);
+        if (wo.z < 0.f) wi.z = -wi.z;
+        pdf = fabsf(wi.z) * kInvPi;
+        if (pdf == 0.f) return false;
+        f = mk(m.albedo[0] * kInvPi, m.albedo[1] * kInvPi, m.albedo[2] * kInvPi);
+        return true;
+    }
+    if (wo.z == 0.f) return false;
+    float a2 = m.alpha * m.alpha;
+    float c2 = (1.0f - ux) / ((a2 - 1.0f) * ux + 1.0f);
+    float ch = sqrtf(fmaxf(c2, 0.f)), sh = sqrtf(fmaxf(1.0f - c2, 0.f));
+    float phi = (2.0f * kPi) * uy;
+    f3 h = mk(sh * cosf(phi), sh * sinf(phi), ch);
+    if (h.z * wo.z < 0.f) h = -h;
+    wi = -wo + (h * 2.0f) * dot(wo, h);
+    if (!same_hemi(wi, wo)) return false;
+    pdf = bsdf_pdf(m, wi, wo);
+    if (pdf == 0.f) return false;
+    f = bsdf_eval(m, wi, wo);
+    return true;
+}
+
+// ---- lights ----
+struct LightView {
+    uint32_t kind;
+    float area;
+    f3 pos, inten, e1, e2, n;
+};
+__device__ __forceinline__ LightView load_light(const DevScene& sc, uint32_t i) {
+    const LightRecord& r = sc.lights[i];
+    LightView l;
+    l.kind = r.kind;
+    l.area = r.area;
+    l.pos = ld3(r.pos);
+    l.inten = ld3(r.inten);
+    l.e1 = ld3(r.e1);
+    l.e2 = ld3(r.e2);
+    l.n = ld3(r.n);
+    return l;
+}
+__device__ __forceinline__ bool light_enabled(const DevScene& sc) {
+    return sc.light_dist != AR_LIGHT_DIST_NONE && sc.num_lights > 0;
+}
+__device__ __forceinline__ void light_select(const DevScene& sc, float u, uint32_t& idx, float& pmf) {
+    const uint32_t n = sc.num_lights;
+    if (sc.light_dist == AR_LIGHT_DIST_UNIFORM) {
+        float s = u * float(n);
+        uint32_t i = s >= 0.f ? uint32_t(s) : 0u;
+        idx = min(i, n - 1);
+        pmf = 1.0f / float(n);
+        return;
+    }
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (sc.light_cdf[mid] < u) lo = mid + 1; else hi = mid;
+    }
+    idx = min(lo, n - 1);
+    pmf = sc.light_pmf[idx];
+}
+__device__ __forceinline__ float light_pmf_of(const DevScene& sc, uint32_t i) {
+    return sc.light_dist == AR_LIGHT_DIST_UNIFORM ? 1.0f / float(sc.num_lights) : sc.light_pmf[i];
+}
+// Light::sample toward `ref`; false when the reference returns None.
+__device__ __forceinline__ bool light_sample(const LightView& l, f3 ref, float ux, float uy, f3& wi, float& dist, f3& li,
+                                             float& pdf) {
+    if (l.kind == AR_LIGHT_POINT) {
+        f3 off = l.pos - ref;
+        float d2 = dot(off, off);
+        float d = sqrtf(d2);
+        if (d < 1e-6f) return false;
+        wi = off / d;
+        dist = d;
+        li = l.inten / d2;
+        pdf = 1.0f;
+        return true;
+    }
+    f3 q = (l.pos + l.e1 * ux) + l.e2 * uy;
+    f3 off = q - ref;
+    float d2 = dot(off, off);
+    float d = sqrtf(d2);
+    if (d < 1e-6f) return false;
+    wi = off / d;
+    float cl = -dot(l.n, wi);
+    if (cl <= 0.f) return false;
+    dist = d;
+    li = l.inten;
+    pdf = d2 / (cl * l.area);
+    return true;
+}
+__device__ __forceinline__ float light_pdf_emission_dir(const LightView& l, f3 dir) {
+    if (l.kind == AR_LIGHT_POINT) return 1.0f / (4.0f * kPi);
+    float c = dot(l.n, dir);
+    return c > 0.f ? c * kInvPi : 0.f;
+}
+
+// ---- camera ----
+__device__ __forceinline__ Ray camera_ray(const CameraDev& c, float u, float v) {
+    f3 dir = ((ld3(c.ll) + ld3(c.hor) * u) + ld3(c.ver) * v) - ld3(c.o);
+    return Ray{ld3(c.o), normalize(dir), 0.001f, FLT_MAX};
+}
+__device__ __forceinline__ float camera_pdf_we(const CameraDev& c, f3 d) {
+    float ct = dot(d, ld3(c.fwd));
+    if (ct <= 0.f) return 0.f;
+    return 1.0f / (((c.area * ct) * ct) * ct);
+}
+
+__device__ __forceinline__ float power_heuristic(float a, float b) {
+    float a2 = a * a, b2 = b * b;
+    return a2 / (a2 + b2);
+}
+
+// Warp-aggregated queue slot allocation; every lane of the warp must call it.
+__device__ __forceinline__ uint32_t warp_alloc(uint32_t* counter, bool pred) {
+    const uint32_t mask = __ballot_sync(0xffffffffu, pred);
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t base = 0;
+    if (mask) {
+        const int leader = __ffs(mask) - 1;
+        if (int(lane) == leader) base = atomicAdd(counter, uint32_t(__popc(mask)));
+        base = __shfl_sync(0xffffffffu, base, leader);
+    }
+    return base + uint32_t(__popc(mask & ((1u << lane) - 1u)));
+}
+
+}  // namespace ar

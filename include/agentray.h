@@ -1,0 +1,283 @@
+/*
+ * agentray.h — C ABI of the B200 light-transport library (libagentray.so).
+ *
+ * This is the drop-in boundary for agent-ray's light-transport hot path.  The
+ * reference crate exposes it as Rust traits; each entry point below names the
+ * reference interface it replaces (paths are inside the agent-ray crate):
+ *
+ *   Integrator::render(&Scene, &dyn Camera, w, h) -> Arc<Film>
+ *       src/integrators/mod.rs:18-26                    -> ar_render
+ *   Scene::new(objects, lights, light_dist)
+ *       src/scene.rs:125-139 (+ SceneObject::new :29-35) -> ar_scene_create
+ *   BLASAccel::build / TLAS::build
+ *       src/accel/bvh.rs:326-344, :395-411               -> ar_scene_build_accel
+ *   Scene::intersect(&Ray) -> Option<(f32, ShadingPoint)> / TLAS::intersect
+ *       src/scene.rs:142-162, src/accel/bvh.rs:413-447   -> ar_trace_closest
+ *   Scene::occluded(&Ray) -> bool
+ *       src/scene.rs:166-168                             -> ar_trace_any
+ *   Film::to_hdr_vec() -> Vec<Vec3A>
+ *       src/film.rs:272-274                              -> the out_rgb buffer of ar_render
+ *
+ * Conventions
+ *   - Every function returns an int status: AR_OK (0) or a negative AR_ERR_*.
+ *     ar_last_error() returns a message for the calling thread's last error.
+ *     No C++ exception crosses this ABI.
+ *   - Scene descriptors hold host pointers; ar_scene_create copies everything
+ *     it needs, so the caller keeps ownership and may free them afterwards.
+ *   - Matrices are 4x4 column-major (glam::Mat4 memory layout).
+ *   - Rays follow the reference Ray::new (src/geometry.rs:12-20): the library
+ *     normalises the direction exactly as glam's Vec3A::normalize does.
+ *   - A context owns one CUDA stream.  A context is externally synchronised:
+ *     one host thread at a time.  Different contexts are independent.
+ *   - Buffers flagged `on_device` are CUDA device pointers on the context's
+ *     device; otherwise they are host pointers (pinned or pageable).
+ */
+#ifndef AGENTRAY_H
+#define AGENTRAY_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AR_ABI_VERSION 1
+
+enum ar_status {
+    AR_OK = 0,
+    AR_ERR_INVALID_ARGUMENT = -1,
+    AR_ERR_CUDA = -2,
+    AR_ERR_OUT_OF_MEMORY = -3,
+    AR_ERR_UNSUPPORTED = -4,
+    AR_ERR_TIMEOUT = -5,
+    AR_ERR_NOT_FOUND = -6,
+    AR_ERR_REJECTED = -7,
+    AR_ERR_INTERNAL = -8
+};
+
+typedef struct ar_context ar_context;
+typedef struct ar_scene ar_scene;
+
+/* ---- scene description (src/primitives/mesh.rs:7-16, src/scene.rs:17-48) ---- */
+
+typedef struct ar_mesh_desc {
+    const float* positions;          /* num_vertices * 3 */
+    const float* normals;            /* num_vertices * 3, or NULL (geometric normal is used) */
+    const uint32_t* indices;         /* num_triangles * 3 */
+    const uint32_t* material_slots;  /* 1 entry (shared slot) or num_triangles entries */
+    uint32_t num_vertices;
+    uint32_t num_triangles;
+    uint32_t num_material_slots;
+    uint32_t _pad;
+} ar_mesh_desc;
+
+/* One SceneObject: a mesh placed by a local->world transform, with its
+ * slot -> material table (src/scene.rs:17-48). */
+typedef struct ar_object_desc {
+    float transform[16];             /* column-major local->world */
+    float inv_transform[16];         /* column-major world->local, used when has_inverse != 0 */
+    const uint32_t* materials;       /* slot -> index into ar_scene_desc.materials */
+    uint32_t mesh;
+    uint32_t num_materials;
+    uint32_t has_inverse;
+    uint32_t _pad;
+} ar_object_desc;
+
+enum ar_material_kind {
+    AR_MATERIAL_LAMBERTIAN = 0,      /* src/surfaces/lambertian.rs */
+    AR_MATERIAL_CONDUCTOR = 1        /* src/surfaces/microfacet.rs:86-152 (GGX) */
+};
+
+typedef struct ar_material_desc {
+    uint32_t kind;
+    int32_t emitter_light;           /* >= 0: this surface is the emitting face of quad light
+                                        `emitter_light` (area-light extension); -1 otherwise */
+    float albedo[3];                 /* Lambertian albedo (constant texture) */
+    float f0[3];                     /* conductor reflectance at normal incidence */
+    float roughness;                 /* conductor GGX alpha, clamped to [1e-3, 1] */
+    float _pad;
+} ar_material_desc;
+
+enum ar_light_kind {
+    AR_LIGHT_POINT = 0,              /* src/lights/point.rs */
+    AR_LIGHT_QUAD = 1                /* one-sided quad area light (extension, see DESIGN) */
+};
+
+typedef struct ar_light_desc {
+    uint32_t kind;
+    uint32_t _pad;
+    float position[3];               /* point: position;  quad: corner */
+    float intensity[3];              /* point: intensity (W/sr); quad: radiance */
+    float edge1[3];                  /* quad only: corner + s*edge1 + t*edge2, normal = edge1 x edge2 */
+    float edge2[3];
+} ar_light_desc;
+
+enum ar_light_distribution {
+    AR_LIGHT_DIST_NONE = 0,
+    AR_LIGHT_DIST_UNIFORM = 1,       /* src/lights.rs:136-159 */
+    AR_LIGHT_DIST_POWER = 2          /* src/lights.rs:171-235 */
+};
+
+typedef struct ar_scene_desc {
+    const ar_mesh_desc* meshes;
+    const ar_object_desc* objects;
+    const ar_material_desc* materials;
+    const ar_light_desc* lights;
+    uint32_t num_meshes;
+    uint32_t num_objects;
+    uint32_t num_materials;
+    uint32_t num_lights;
+    uint32_t light_distribution;
+    uint32_t _pad;
+} ar_scene_desc;
+
+/* PinholeCamera::from_lookat (src/cameras.rs:91-123). */
+typedef struct ar_camera_desc {
+    float lookfrom[3];
+    float lookat[3];
+    float vup[3];
+    float vfov_deg;
+    float aspect;
+} ar_camera_desc;
+
+/* ---- integrator configuration (config structs of src/integrators/) ---- */
+
+enum ar_integrator_kind {
+    AR_INTEGRATOR_PT = 0,            /* PathTracerConfig, src/integrators/path_tracer.rs:18-31 */
+    AR_INTEGRATOR_BDPT = 1,          /* BdptConfig, src/integrators/bidirectional_path_tracer.rs:102-133 */
+    AR_INTEGRATOR_GDPT = 2           /* GdptConfig, src/integrators/gradient_domain_pt.rs:47-76 */
+};
+enum ar_mis_mode { AR_MIS_POWER = 0, AR_MIS_UNIFORM = 1 };
+enum ar_poisson_solver {
+    AR_POISSON_SOR = 0,              /* the reference red-black SOR, gradient_domain_pt.rs:449-630 */
+    AR_POISSON_CG = 1                /* FP32 conjugate gradient with FP64 residual refinement */
+};
+enum ar_film_precision { AR_FILM_F32 = 0, AR_FILM_F64 = 1 };
+
+typedef struct ar_integrator_cfg {
+    uint32_t integrator;             /* ar_integrator_kind */
+    uint32_t spp;
+    uint32_t max_depth;
+    uint32_t rr_depth;
+    uint32_t mis_mode;               /* BDPT */
+    float mis_beta;                  /* BDPT */
+    float alpha;                     /* GDPT screening weight */
+    uint32_t poisson_iterations;     /* GDPT SOR iterations / CG iteration cap */
+    float sor_omega;                 /* GDPT SOR relaxation */
+    uint32_t poisson_solver;         /* ar_poisson_solver */
+    double poisson_tolerance;        /* CG: relative residual target (FP64) */
+    uint64_t seed;                   /* sampler key; 0 reproduces the default stream */
+    uint32_t film_precision;         /* ar_film_precision */
+    uint32_t _pad;
+} ar_integrator_cfg;
+
+/* ---- ray batches (src/geometry.rs:3-20, src/accel/bvh.rs:10-20) ---- */
+
+typedef struct ar_ray_batch {
+    const float* org_tmin;           /* count * 4: origin.xyz, t_min */
+    const float* dir_tmax;           /* count * 4: direction.xyz (normalised by the library), t_max */
+    uint64_t count;
+    uint32_t on_device;
+    uint32_t _pad;
+} ar_ray_batch;
+
+/* RayHit (src/accel/bvh.rs:10-20): t, barycentric (u, v) and prim_id; miss =
+ * t = +inf, prim_id = inst_id = 0xFFFFFFFF (RayHit::INVALID_ID). */
+typedef struct ar_hit {
+    float t;
+    float u;
+    float v;
+    uint32_t prim_id;
+} ar_hit;
+
+typedef struct ar_accel_opts {
+    uint32_t max_leaf_size;          /* 1..3 triangles per wide-BVH leaf (default 3) */
+    uint32_t sah_bins;               /* binned SAH bins (default 32) */
+    uint32_t build_threads;          /* host threads for the build (0 = all cores) */
+    uint32_t _pad;
+} ar_accel_opts;
+
+typedef struct ar_scene_stats {
+    uint64_t num_triangles;
+    uint64_t num_instances;
+    uint64_t num_blas_nodes;         /* 8-wide nodes across all meshes */
+    uint64_t num_tlas_nodes;
+    uint64_t device_bytes;           /* total device memory held by the scene */
+    uint32_t max_stack_depth;        /* worst-case traversal stack entries */
+    uint32_t _pad;
+    double build_seconds;
+} ar_scene_stats;
+
+/* ---- entry points ---- */
+
+const char* ar_last_error(void);
+int ar_abi_version(void);
+
+int ar_context_create(int device, ar_context** out);
+int ar_context_destroy(ar_context* ctx);
+/* Use the caller's CUDA stream (cudaStream_t passed as void*) instead of the
+ * context's own; NULL restores the context stream. */
+int ar_context_set_stream(ar_context* ctx, void* cuda_stream);
+int ar_context_synchronize(ar_context* ctx);
+
+int ar_scene_create(ar_context* ctx, const ar_scene_desc* desc, ar_scene** out);
+int ar_scene_destroy(ar_scene* scene);
+/* (Re)build the acceleration structures with explicit options.  ar_scene_create
+ * already builds with defaults. */
+int ar_scene_build_accel(ar_context* ctx, ar_scene* scene, const ar_accel_opts* opts);
+int ar_scene_get_stats(const ar_scene* scene, ar_scene_stats* out);
+
+/* Closest hit for every ray (Scene::intersect / TLAS::intersect).  `hits` and
+ * `inst_ids` have `rays->count` entries and live where `out_on_device` says. */
+int ar_trace_closest(ar_context* ctx, const ar_scene* scene, const ar_ray_batch* rays,
+                     ar_hit* hits, uint32_t* inst_ids, uint32_t out_on_device);
+/* Occlusion for every ray (Scene::occluded): occluded[i] = 1 if any triangle is
+ * hit with t in [t_min, t_max]. */
+int ar_trace_any(ar_context* ctx, const ar_scene* scene, const ar_ray_batch* rays,
+                 uint8_t* occluded, uint32_t out_on_device);
+
+/* Integrator::render: W*H*3 linear HDR floats, row-major from the top-left,
+ * already divided by spp (Film::to_hdr_vec). */
+int ar_render(ar_context* ctx, const ar_scene* scene, const ar_camera_desc* camera,
+              const ar_integrator_cfg* cfg, uint32_t width, uint32_t height,
+              float* out_rgb, uint32_t out_on_device);
+
+/* screened_poisson_reconstruct (src/integrators/gradient_domain_pt.rs:449-630):
+ * reconstructs an image from interleaved-RGB primal and forward-difference
+ * gradient films (W*H*3 f32 each) with cfg->alpha and cfg->poisson_solver
+ * (SOR: cfg->poisson_iterations sweeps with cfg->sor_omega; CG: to
+ * cfg->poisson_tolerance).  `rel_residual` (optional, host) receives the final
+ * FP64 relative residual of the CG solver (-1 for SOR). */
+int ar_poisson_reconstruct(ar_context* ctx, const ar_integrator_cfg* cfg, uint32_t width, uint32_t height,
+                           const float* primal, const float* grad_x, const float* grad_y, float* out,
+                           uint32_t on_device, double* rel_residual);
+
+/* ---- instrumentation (no counterpart in the reference) ---- */
+
+/* Work counters of the last ar_render on this context. */
+typedef struct ar_render_stats {
+    uint64_t path_samples;           /* camera samples (GDPT: base samples) */
+    uint64_t paths;                  /* traced paths (GDPT: base + offsets) */
+    uint64_t extend_rays;            /* closest-hit queries */
+    uint64_t shadow_rays;            /* any-hit queries */
+    uint64_t extend_launches;
+    uint64_t shadow_launches;
+} ar_render_stats;
+int ar_get_render_stats(const ar_context* ctx, ar_render_stats* out);
+
+/* When enabled, every kernel launch of the context is bracketed by CUDA events
+ * on the context stream; ar_profile_read returns, per kernel name, the launch
+ * count and summed device milliseconds since the last reset. */
+int ar_profile_enable(ar_context* ctx, int enable);
+int ar_profile_reset(ar_context* ctx);
+/* names: '\n'-separated kernel names written into `names` (capacity bytes);
+ * ms/launches: arrays of `*count` entries (capacity given in *count on entry). */
+int ar_profile_read(ar_context* ctx, char* names, uint32_t capacity, double* ms, uint64_t* launches,
+                    uint32_t* count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AGENTRAY_H */

@@ -1,0 +1,154 @@
+"""ctypes binding of the CPU restatement oracle (oracle/_build/liboracle_agentray.so).
+
+TEST INFRASTRUCTURE ONLY.  Imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py as the checker; never by the product path.
+
+PARITY UNPINNED: agent-ray is Rust, has no tests or golden vectors, and cannot
+be built here; the oracle is a line-by-line C++ restatement (see ar_*.hpp).
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle_agentray.so")
+
+SAMPLER_XOSHIRO = 0
+SAMPLER_COUNTER = 1
+
+_lib = None
+
+
+def build():
+    subprocess.check_call(["make", "-s", "-C", HERE])
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        lb = C.CDLL(LIB_PATH)
+        vp, u32, u64 = C.c_void_p, C.c_uint32, C.c_uint64
+        lb.oracle_scene_create.argtypes = [vp, C.c_int, C.POINTER(vp)]
+        lb.oracle_scene_destroy.argtypes = [vp]
+        lb.oracle_scene_destroy.restype = None
+        lb.oracle_trace.argtypes = [vp, vp, vp, u64, C.c_int, vp, vp, vp, vp, vp, vp, vp, u32]
+        lb.oracle_render.argtypes = [vp, vp, vp, u32, u32, u32, u32, vp, vp, vp, vp]
+        lb.oracle_poisson_sor_f32.argtypes = [u32, u32, vp, vp, vp, C.c_float, u32, C.c_float, vp]
+        lb.oracle_poisson_exact_f64.argtypes = [u32, u32, vp, vp, vp, C.c_double, C.c_double, u32, vp, vp]
+        lb.oracle_counter_u01.argtypes = [u64, u32, u32, u32, u32, vp]
+        lb.oracle_xoshiro_f32.argtypes = [u32, u32, u32, vp]
+        lb.oracle_blas_stats.argtypes = [vp, u32, vp]
+        _lib = lb
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+class OracleScene:
+    def __init__(self, scene_data, precision=32):
+        self.precision = precision
+        desc, keep = scene_data.desc()
+        self.h = C.c_void_p()
+        lib().oracle_scene_create(C.addressof(desc), precision, C.byref(self.h))
+        del keep
+
+    def close(self):
+        if self.h:
+            lib().oracle_scene_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def trace_closest(self, org_tmin, dir_tmax, threads=0, stats=False):
+        n = org_tmin.shape[0]
+        ot = np.ascontiguousarray(org_tmin, np.float32)
+        dt = np.ascontiguousarray(dir_tmax, np.float32)
+        t = np.empty(n, np.float32)
+        u = np.empty(n, np.float32)
+        v = np.empty(n, np.float32)
+        prim = np.empty(n, np.uint32)
+        inst = np.empty(n, np.uint32)
+        st = np.zeros(3, np.uint64) if stats else None
+        lib().oracle_trace(self.h, _p(ot), _p(dt), n, 0, _p(t), _p(u), _p(v), _p(prim), _p(inst), None, _p(st),
+                           threads)
+        out = dict(t=t, u=u, v=v, prim=prim, inst=inst)
+        if stats:
+            out["stats"] = dict(nodes=int(st[0]), tris=int(st[1]), instances=int(st[2]))
+        return out
+
+    def trace_any(self, org_tmin, dir_tmax, threads=0):
+        n = org_tmin.shape[0]
+        ot = np.ascontiguousarray(org_tmin, np.float32)
+        dt = np.ascontiguousarray(dir_tmax, np.float32)
+        occ = np.empty(n, np.uint8)
+        lib().oracle_trace(self.h, _p(ot), _p(dt), n, 1, None, None, None, None, None, _p(occ), None, threads)
+        return occ
+
+    def render(self, camera, cfg, width, height, sampler=SAMPLER_COUNTER, threads=0, moments=False, gdpt_films=False):
+        """Returns the (H, W, 3) float64 image; with moments=True also the per-pixel
+        mean squared sample radiance (PT) or, for GDPT, with gdpt_films=True the
+        (primal, dx, dy) films."""
+        cam = camera.desc()
+        n = width * height * 3
+        out = np.empty(n, np.float64)
+        a0 = np.empty(n, np.float64) if (moments or gdpt_films) else None
+        a1 = np.empty(n, np.float64) if gdpt_films else None
+        a2 = np.empty(n, np.float64) if gdpt_films else None
+        rc = lib().oracle_render(self.h, C.addressof(cam), C.addressof(cfg), width, height, sampler, threads,
+                                 _p(out), _p(a0), _p(a1), _p(a2))
+        if rc != 0:
+            raise RuntimeError("oracle_render failed")
+        img = out.reshape(height, width, 3)
+        if gdpt_films:
+            return img, a0.reshape(height, width, 3), a1.reshape(height, width, 3), a2.reshape(height, width, 3)
+        if moments:
+            return img, a0.reshape(height, width, 3)
+        return img
+
+    def blas_stats(self, mesh=0):
+        o = np.zeros(3, np.uint64)
+        lib().oracle_blas_stats(self.h, mesh, _p(o))
+        return dict(nodes=int(o[0]), leaves=int(o[1]), depth=int(o[2]))
+
+
+def poisson_sor_f32(primal, gx, gy, alpha, iters, omega):
+    h, w, _ = primal.shape
+    p = np.ascontiguousarray(primal, np.float32)
+    x = np.ascontiguousarray(gx, np.float32)
+    y = np.ascontiguousarray(gy, np.float32)
+    out = np.empty_like(p)
+    lib().oracle_poisson_sor_f32(w, h, _p(p), _p(x), _p(y), alpha, iters, omega, _p(out))
+    return out
+
+
+def poisson_exact_f64(primal, gx, gy, alpha, tol=1e-12, max_iters=10000):
+    h, w, _ = primal.shape
+    p = np.ascontiguousarray(primal, np.float64)
+    x = np.ascontiguousarray(gx, np.float64)
+    y = np.ascontiguousarray(gy, np.float64)
+    out = np.empty_like(p)
+    rr = np.zeros(1, np.float64)
+    lib().oracle_poisson_exact_f64(w, h, _p(p), _p(x), _p(y), alpha, tol, max_iters, _p(out), _p(rr))
+    return out, float(rr[0])
+
+
+def counter_u01(seed, pixel, sample, dim0, n):
+    out = np.empty(n, np.float32)
+    lib().oracle_counter_u01(seed, pixel, sample, dim0, n, _p(out))
+    return out
+
+
+def xoshiro_f32(px, py, n):
+    out = np.empty(n, np.float32)
+    lib().oracle_xoshiro_f32(px, py, n, _p(out))
+    return out

@@ -1,0 +1,202 @@
+"""GPU parity: libagentray (CUDA, sm_100a) against the CPU oracle on the same
+seeded inputs.  Bars:
+  * BVH: closest-hit (inst_id, prim_id) equal to the oracle's restatement of
+    the reference traversal; a mismatch is tolerated only for ties
+    (|t_gpu - t_ref| <= 1e-6 * max(1, t)) or hits within 1e-6 of a triangle edge
+    in barycentric terms.  Any-hit booleans likewise.
+  * Images: same counter-based sample stream -> per-pixel agreement (rel. 1e-3)
+    on >= 98% of pixels and mean within 0.5%; an independent-seed run must
+    pass a per-pixel z-test (|z| > 4 on at most 0.5% of pixels).
+  * Red-black SOR: bit-exact to the oracle.
+"""
+import numpy as np
+import pytest
+
+import agentray
+import agentray.scenes as S
+import oracle as O
+from agentray import _abi as A
+from agentray.scene_data import integrator_cfg
+
+pytestmark = pytest.mark.gpu
+
+INVALID = 0xFFFFFFFF
+
+
+def _edge_case(u, v, eps=1e-6):
+    return (u <= eps) | (v <= eps) | (u + v >= 1 - eps)
+
+
+def _compare_hits(gpu_hits, gpu_inst, ref, eps_t=1e-6):
+    g_prim = gpu_hits[:, 3].view(np.uint32)
+    g_t = gpu_hits[:, 0]
+    same = (g_prim == ref["prim"]) & (gpu_inst == ref["inst"])
+    both = (g_prim != INVALID) & (ref["prim"] != INVALID)
+    tie = both & (np.abs(g_t - ref["t"]) <= eps_t * np.maximum(1.0, np.abs(ref["t"])))
+    edge = _edge_case(ref["u"], ref["v"]) | _edge_case(gpu_hits[:, 1], gpu_hits[:, 2])
+    bad = ~(same | tie | edge)
+    return same, bad
+
+
+def test_closest_hit_soup(ctx):
+    sc = S.triangle_soup(200_000, seed=2)
+    g = agentray.Scene(ctx, sc)
+    osc = O.OracleScene(sc)
+    ot, dt = S.soup_rays(200_000, seed=3)
+    hits, inst = g.trace_closest(ot, dt)
+    ref = osc.trace_closest(ot, dt)
+    same, bad = _compare_hits(hits, inst, ref)
+    assert bad.sum() == 0, f"{bad.sum()} mismatches"
+    assert same.mean() > 0.999
+    # exact t/u/v where the same triangle is hit
+    m = same & (ref["prim"] != INVALID)
+    np.testing.assert_array_equal(hits[m, 0], ref["t"][m])
+    np.testing.assert_array_equal(hits[m, 1], ref["u"][m])
+    np.testing.assert_array_equal(hits[m, 2], ref["v"][m])
+
+
+def test_any_hit_soup(ctx):
+    sc = S.triangle_soup(100_000, seed=7)
+    g = agentray.Scene(ctx, sc)
+    osc = O.OracleScene(sc)
+    ot, dt = S.soup_rays(100_000, seed=8, tmax=0.25)
+    occ = g.trace_any(ot, dt)
+    ref = osc.trace_any(ot, dt)
+    mism = occ != ref
+    if mism.any():
+        r = osc.trace_closest(ot[mism], dt[mism])
+        assert np.all(_edge_case(r["u"], r["v"]) | (np.abs(r["t"] - 0.25) < 1e-6)), f"{mism.sum()} mismatches"
+    assert (occ == ref).mean() > 0.9999
+
+
+def test_closest_hit_instanced_room(ctx):
+    sc, cam = S.room(seed=4, sphere_levels=(3, 3, 2, 2), n_boxes=120)
+    g = agentray.Scene(ctx, sc)
+    osc = O.OracleScene(sc)
+    rng = np.random.default_rng(9)
+    n = 100_000
+    ot = np.zeros((n, 4), np.float32)
+    dt = np.zeros((n, 4), np.float32)
+    ot[:, :3] = rng.uniform((0.1, 0.1, 0.1), (9.9, 4.9, 9.9), (n, 3))
+    ot[:, 3] = 1e-4
+    d = rng.normal(size=(n, 3))
+    dt[:, :3] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    dt[:, 3] = np.inf
+    hits, inst = g.trace_closest(ot, dt)
+    ref = osc.trace_closest(ot, dt)
+    same, bad = _compare_hits(hits, inst, ref)
+    assert bad.sum() == 0, f"{bad.sum()} mismatches"
+    assert same.mean() > 0.999
+    assert g.stats()["num_instances"] == len(sc.objects)
+
+
+def test_empty_and_degenerate_rays(ctx):
+    sc = S.triangle_soup(1000, seed=1)
+    g = agentray.Scene(ctx, sc)
+    osc = O.OracleScene(sc)
+    hits, inst = g.trace_closest(np.zeros((0, 4), np.float32), np.zeros((0, 4), np.float32))
+    assert hits.shape == (0, 4)
+    # axis-aligned directions (zero components) and a t-range that excludes all hits
+    ot, dt = S.soup_rays(5000, seed=4)
+    dt[:2500, :3] = np.eye(3, dtype=np.float32)[np.arange(2500) % 3] * np.where(np.arange(2500) % 2, 1, -1)[:, None]
+    dt[4000:, 3] = 1e-5
+    hits, inst = g.trace_closest(ot, dt)
+    ref = osc.trace_closest(ot, dt)
+    same, bad = _compare_hits(hits, inst, ref)
+    assert bad.sum() == 0
+    assert np.all(hits[4000:, 3].view(np.uint32) == INVALID)
+
+
+def _render_gpu(ctx, sc, cam, cfg, w, h):
+    g = agentray.Scene(ctx, sc)
+    out = np.empty(w * h * 3, np.float32)
+    import ctypes as C
+    agentray.check(agentray.lib().ar_render(ctx.handle, g.handle, C.byref(cam.desc()), C.byref(cfg), w, h,
+                                            out.ctypes.data, 0))
+    return out.reshape(h, w, 3).astype(np.float64)
+
+
+@pytest.mark.parametrize("point_light", [False, True])
+def test_pt_same_stream_matches_oracle(ctx, point_light):
+    sc, cam = S.cornell_box(1, point_light=point_light)
+    cfg = integrator_cfg(A.INTEGRATOR_PT, spp=16, max_depth=8, rr_depth=3, seed=5)
+    w = h = 64
+    gpu = _render_gpu(ctx, sc, cam, cfg, w, h)
+    ref = O.OracleScene(sc).render(cam, cfg, w, h, sampler=O.SAMPLER_COUNTER)
+    close = np.abs(gpu - ref) <= 1e-3 * np.maximum(1.0, np.abs(ref))
+    assert close.all(axis=2).mean() >= 0.98, close.all(axis=2).mean()
+    assert abs(gpu.mean() - ref.mean()) / ref.mean() < 5e-3
+
+
+def welch_fail_fraction(a_reps, b_reps, thresh=4.5):
+    """Per-pixel Welch t-test on replicate means (independent seeds).  Pixels
+    with zero spread on both sides must agree to 1e-5 relative."""
+    ma, mb = a_reps.mean(0), b_reps.mean(0)
+    va, vb = a_reps.var(0, ddof=1), b_reps.var(0, ddof=1)
+    k = a_reps.shape[0]
+    se = np.sqrt(va / k + vb / k)
+    zero = se == 0
+    t = np.where(zero, 0.0, (ma - mb) / np.where(zero, 1.0, se))
+    exact_bad = zero & (np.abs(ma - mb) > 1e-5 * np.maximum(1.0, np.abs(mb)))
+    return float(((np.abs(t) > thresh) | exact_bad).mean())
+
+
+def test_pt_statistically_equal_to_independent_oracle(ctx):
+    # GPU and oracle on disjoint seeds: 8 replicates of 16 spp each.
+    sc, cam = S.cornell_box(1)
+    w = h = 48
+    osc = O.OracleScene(sc)
+    g = np.stack([_render_gpu(ctx, sc, cam, integrator_cfg(A.INTEGRATOR_PT, spp=16, seed=100 + k), w, h)
+                  for k in range(8)])
+    r = np.stack([osc.render(cam, integrator_cfg(A.INTEGRATOR_PT, spp=16, seed=200 + k), w, h,
+                             sampler=O.SAMPLER_COUNTER) for k in range(8)])
+    assert welch_fail_fraction(g, r) < 0.005
+    # the reference's own sampler (xoshiro256++ per-pixel stream) agrees in distribution too
+    x = np.stack([osc.render(cam, integrator_cfg(A.INTEGRATOR_PT, spp=16, seed=300 + k), w, h,
+                             sampler=O.SAMPLER_XOSHIRO) for k in range(8)])
+    assert welch_fail_fraction(g, x) < 0.005
+
+
+def test_pt_film_f64_matches_f32(ctx):
+    sc, cam = S.cornell_box(1)
+    a = _render_gpu(ctx, sc, cam, integrator_cfg(A.INTEGRATOR_PT, spp=8, seed=3, film_precision=A.FILM_F32), 32, 32)
+    b = _render_gpu(ctx, sc, cam, integrator_cfg(A.INTEGRATOR_PT, spp=8, seed=3, film_precision=A.FILM_F64), 32, 32)
+    np.testing.assert_allclose(a, b, rtol=1e-5, atol=1e-6)
+
+
+def test_sor_bit_exact(ctx):
+    rng = np.random.default_rng(1)
+    h, w = 37, 53
+    primal = rng.uniform(0.0, 2.0, (h, w, 3)).astype(np.float32)
+    gx = (rng.normal(size=(h, w, 3)) * 0.2).astype(np.float32)
+    gy = (rng.normal(size=(h, w, 3)) * 0.2).astype(np.float32)
+    gx[:, -1] = 0
+    gy[-1, :] = 0
+    ref = O.poisson_sor_f32(primal, gx, gy, 0.2, 200, 1.6)
+    out, _ = agentray.poisson_reconstruct(ctx, primal, gx, gy, 0.2, A.POISSON_SOR, 200, 1.6)
+    np.testing.assert_array_equal(out, ref)
+
+
+def test_cg_fp64_refined_reaches_tolerance(ctx):
+    rng = np.random.default_rng(2)
+    h, w = 96, 128
+    primal = rng.uniform(0.0, 2.0, (h, w, 3)).astype(np.float32)
+    gx = (rng.normal(size=(h, w, 3)) * 0.2).astype(np.float32)
+    gy = (rng.normal(size=(h, w, 3)) * 0.2).astype(np.float32)
+    gx[:, -1] = 0
+    gy[-1, :] = 0
+    exact, _ = O.poisson_exact_f64(primal, gx, gy, 0.2)
+    out, res = agentray.poisson_reconstruct(ctx, primal, gx, gy, 0.2, A.POISSON_CG, 2000, 1.6, 1e-6)
+    assert 0 <= res <= 1e-6
+    np.testing.assert_allclose(out, np.maximum(exact, 0), atol=5e-5 * np.abs(exact).max())
+
+
+def test_gdpt_same_stream_matches_oracle(ctx):
+    sc, cam = S.cornell_box(1)
+    cfg = integrator_cfg(A.INTEGRATOR_GDPT, spp=8, max_depth=6, seed=2)
+    w, h = 48, 40
+    gpu = _render_gpu(ctx, sc, cam, cfg, w, h)
+    ref = O.OracleScene(sc).render(cam, cfg, w, h, sampler=O.SAMPLER_COUNTER)
+    assert abs(gpu.mean() - ref.mean()) / ref.mean() < 1e-2
+    close = np.abs(gpu - ref) <= 2e-2 * np.maximum(1.0, np.abs(ref))
+    assert close.all(axis=2).mean() >= 0.95

@@ -120,8 +120,12 @@ struct ar_context {
     ar::DevBuf stats_d;       // uint64[8]: render work counters
     ar::Workspace work;       // wavefront state
     ar::Workspace io;         // staging for host <-> device transfers
+    ar::Workspace films;      // accumulation films of the current render
+    ar::Workspace solver;     // Poisson solver buffers
     ar::Profiler prof;
+    uint64_t* stats_h = nullptr;  // pinned copy of stats_d, valid after a sync
     ar_render_stats last_stats{};
+    bool stats_pending = false;
 };
 
 struct ar_scene {

@@ -1,0 +1,635 @@
+// Wavefront bidirectional path tracer (BidirectionalPathTracer::render,
+// src/integrators/bidirectional_path_tracer.rs:1221-1357).
+//
+// Stages per chunk of camera samples:
+//   generate   camera vertex z0 + primary ray, light vertex y0 + emitted ray
+//   [extend -> vertex] x max_depth
+//              both subpaths of every sample trace in one wavefront; each hit
+//              appends a vertex (area-measure pdf_fwd) and retroactively sets
+//              pdf_rev of the previous vertex (:338-559)
+//   connect    one thread per sample enumerates the (s, t) strategies with
+//              s + t <= max_depth + 2, evaluates the unweighted contribution
+//              and the power-heuristic MIS weight (FP64 ratio walk, :594-770)
+//              and emits one shadow ray per candidate (:782-1155)
+//   shadow     any-hit test; visible contributions go to the film (s >= 2: the
+//              sample's pixel; s = 1: the projected splat pixel)
+// Vertices are stored SoA by (subpath, depth, sample) so each stage reads
+// coalesced 16-byte records.  Quad-light strategies (t = 0 and area-light t = 1)
+// are the same extension the oracle implements.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "ar_shading.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace ar {
+
+namespace {
+
+constexpr uint32_t kTypeSurface = 0, kTypeCamera = 1, kTypeLight = 2;
+
+struct BdParams {
+    DevScene sc;
+    CameraDev cam;
+    uint32_t width, height, spp, max_depth, rr_depth, mis_mode;
+    float mis_beta;
+    uint32_t film64;
+    uint64_t seed;
+    uint64_t sample_begin;
+    uint32_t nsamples;  // samples in this chunk
+    uint32_t maxv;      // vertices per subpath (max_depth + 1)
+    float inv_spp;
+    void* film;
+    // vertices: index ((sub * maxv + k) * nsamples + si)
+    float4* va;  // p.xyz, pdf_fwd
+    float4* vb;  // n.xyz, pdf_rev
+    float4* vc;  // thr.xyz, info (type << 30 | delta << 29 | index)
+    uint8_t* nv; // [sub * nsamples + si]
+    // tracing state per subpath q = 2 * si + sub
+    float4* thr;     // thr.xyz, previous directional pdf
+    uint32_t* dim;
+    float4* ray_o[2];
+    float4* ray_d[2];
+    uint32_t* qpath[2];
+    float4* hit;
+    uint32_t* hit_inst;
+    // connection shadow queue
+    float4* sh_o;
+    float4* sh_d;  // dir.xyz, tmax
+    float4* sh_c;  // contribution.xyz, pixel bits
+    uint32_t sh_cap;
+    uint32_t* counts;  // [0..max_depth]: rays per bounce; [64]: shadow rays; [65]: overflow flag
+};
+
+__device__ __forceinline__ size_t vidx(const BdParams& P, uint32_t sub, uint32_t k, uint32_t si) {
+    return (size_t(sub) * P.maxv + k) * P.nsamples + si;
+}
+
+struct Vtx {
+    f3 p, n, thr;
+    float pdf_fwd, pdf_rev;
+    uint32_t type, index;
+    bool delta;
+};
+
+__device__ __forceinline__ Vtx load_vtx(const BdParams& P, uint32_t sub, uint32_t k, uint32_t si) {
+    const size_t i = vidx(P, sub, k, si);
+    const float4 a = P.va[i], b = P.vb[i], c = P.vc[i];
+    Vtx v;
+    v.p = mk(a.x, a.y, a.z);
+    v.pdf_fwd = a.w;
+    v.n = mk(b.x, b.y, b.z);
+    v.pdf_rev = b.w;
+    v.thr = mk(c.x, c.y, c.z);
+    const uint32_t info = __float_as_uint(c.w);
+    v.type = info >> 30;
+    v.delta = (info >> 29) & 1u;
+    v.index = info & 0x1fffffffu;
+    return v;
+}
+
+__device__ __forceinline__ void store_vtx(const BdParams& P, uint32_t sub, uint32_t k, uint32_t si, f3 p, f3 n, f3 thr,
+                                          float pdf_fwd, uint32_t type, bool delta, uint32_t index) {
+    const size_t i = vidx(P, sub, k, si);
+    P.va[i] = make_float4(p.x, p.y, p.z, pdf_fwd);
+    P.vb[i] = make_float4(n.x, n.y, n.z, 0.f);
+    P.vc[i] = make_float4(thr.x, thr.y, thr.z,
+                          __uint_as_float((type << 30) | (delta ? (1u << 29) : 0u) | (index & 0x1fffffffu)));
+}
+
+// pdf_solid_angle_to_area (:305-314) and geometry_term (:318-328)
+__device__ __forceinline__ float pdf_sa_to_area(float pdf, f3 from, f3 to, f3 n_to) {
+    const f3 d = to - from;
+    const float d2 = dot(d, d);
+    if (d2 < 1e-12f) return 0.f;
+    const f3 dir = d / sqrtf(d2);
+    return pdf * fabsf(dot(n_to, dir)) / d2;
+}
+__device__ __forceinline__ float geometry_term(f3 pa, f3 na, f3 pb, f3 nb) {
+    const f3 d = pb - pa;
+    const float d2 = dot(d, d);
+    if (d2 < 1e-12f) return 0.f;
+    const f3 dir = d / sqrtf(d2);
+    return fabsf(dot(na, dir)) * fabsf(dot(nb, -dir)) / d2;
+}
+
+__device__ __forceinline__ f3 uniform_sphere(float ux, float uy) {
+    const float ct = 1.0f - 2.0f * ux;
+    const float st = sqrtf(fmaxf(1.0f - ct * ct, 0.0f));
+    const float phi = (2.0f * kPi) * uy;
+    return mk(st * cosf(phi), st * sinf(phi), ct);
+}
+
+__device__ __forceinline__ bool mis_delta(const Vtx& v) { return v.type == kTypeSurface && v.delta; }
+
+// mis_weight (:594-770) with the area-light extension for the t == 1 step.
+__device__ float mis_weight(const BdParams& P, uint32_t si, uint32_t S, uint32_t T, uint32_t s, uint32_t t,
+                            float pdf_cc, float pdf_cl) {
+    if (P.mis_mode == AR_MIS_UNIFORM) {
+        const uint32_t len = s + t;
+        uint32_t count = 0;
+        for (uint32_t t2 = 0; t2 <= min(len, T); ++t2) {
+            const uint32_t s2 = len - t2;
+            if (s2 > S || s2 + t2 < 2 || s2 == 0) continue;
+            count++;
+        }
+        return count == 0 ? 1.0f : 1.0f / float(count);
+    }
+    if (s + t == 2) return 1.0f;
+    const double beta = double(P.mis_beta);
+    auto pw = [&](double r) { return beta == 2.0 ? r * r : pow(r, beta); };
+    double sum = 0.0;
+    {
+        double ri = 1.0;
+        if (s >= 1) {
+            const Vtx v = load_vtx(P, 0, s - 1, si);
+            ri *= double(pdf_cc) / double(fmaxf(v.pdf_fwd, 1e-30f));
+            const bool pd = s >= 2 ? mis_delta(load_vtx(P, 0, s - 2, si)) : true;
+            if (!mis_delta(v) && !pd) sum += pw(fabs(ri));
+        }
+        for (uint32_t i = s; i-- > 1;) {
+            const Vtx v = load_vtx(P, 0, i, si);
+            ri *= double(fmaxf(v.pdf_rev, 0.f)) / double(fmaxf(v.pdf_fwd, 1e-30f));
+            const bool pd = mis_delta(load_vtx(P, 0, i - 1, si));
+            if (!mis_delta(v) && !pd) sum += pw(fabs(ri));
+        }
+    }
+    {
+        double ri = 1.0;
+        if (t >= 1) {
+            const Vtx v = load_vtx(P, 1, t - 1, si);
+            ri *= double(pdf_cl) / double(fmaxf(v.pdf_fwd, 1e-30f));
+            bool pd;
+            if (t >= 2) {
+                pd = mis_delta(load_vtx(P, 1, t - 2, si));
+            } else {
+                const Vtx y0 = load_vtx(P, 1, 0, si);
+                pd = P.sc.lights[y0.index].kind == AR_LIGHT_POINT;
+            }
+            if (!mis_delta(v) && !pd) sum += pw(fabs(ri));
+        }
+        for (uint32_t i = t; i-- > 1;) {
+            const Vtx v = load_vtx(P, 1, i, si);
+            ri *= double(fmaxf(v.pdf_rev, 0.f)) / double(fmaxf(v.pdf_fwd, 1e-30f));
+            const bool pd = mis_delta(load_vtx(P, 1, i - 1, si));
+            if (!mis_delta(v) && !pd) sum += pw(fabs(ri));
+        }
+    }
+    return float(1.0 / (1.0 + sum));
+}
+
+__device__ __forceinline__ void film_add(const BdParams& P, uint32_t pix, f3 v) {
+    if (P.film64) {
+        double* f = static_cast<double*>(P.film) + 3 * size_t(pix);
+        atomicAdd(f, double(v.x));
+        atomicAdd(f + 1, double(v.y));
+        atomicAdd(f + 2, double(v.z));
+    } else {
+        float* f = static_cast<float*>(P.film) + 3 * size_t(pix);
+        atomicAdd(f, v.x);
+        atomicAdd(f + 1, v.y);
+        atomicAdd(f + 2, v.z);
+    }
+}
+
+__device__ __forceinline__ void push_shadow(const BdParams& P, f3 o, f3 d, float tmax, f3 c, uint32_t pix) {
+    cg::coalesced_group g = cg::coalesced_threads();
+    uint32_t base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(&P.counts[64], g.size());
+    base = g.shfl(base, 0);
+    const uint32_t slot = base + g.thread_rank();
+    if (slot >= P.sh_cap) {
+        atomicExch(&P.counts[65], 1u);
+        return;
+    }
+    P.sh_o[slot] = make_float4(o.x, o.y, o.z, 0.f);
+    P.sh_d[slot] = make_float4(d.x, d.y, d.z, tmax);
+    P.sh_c[slot] = make_float4(c.x, c.y, c.z, __uint_as_float(pix));
+}
+
+__global__ void __launch_bounds__(256) k_bd_generate(BdParams P) {
+    const uint32_t npix = P.width * P.height;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < 2 * P.nsamples; base += gridDim.x * blockDim.x) {
+        const uint32_t q = base + threadIdx.x;
+        bool live = q < 2 * P.nsamples;
+        const uint32_t si = q >> 1, sub = q & 1u;
+        Ray r{};
+        if (live) {
+            const uint64_t g = P.sample_begin + si;
+            const uint32_t pixel = uint32_t(g % npix), sample = uint32_t(g / npix);
+            const uint64_t key = counter_key(P.seed, pixel, sample);
+            if (sub == 0) {
+                const float jx = counter_u01(key, 0), jy = counter_u01(key, 1);
+                const uint32_t px = pixel % P.width, py = pixel / P.width;
+                r = camera_ray(P.cam, (float(px) + jx) / float(P.width), 1.0f - (float(py) + jy) / float(P.height));
+                store_vtx(P, 0, 0, si, ld3(P.cam.o), r.d, mk(1.f, 1.f, 1.f), 1.0f, kTypeCamera, true, 0);
+                P.nv[si] = 1;
+                P.thr[q] = make_float4(1.f, 1.f, 1.f, camera_pdf_we(P.cam, r.d));
+                P.dim[q] = 2;
+            } else if (light_enabled(P.sc)) {
+                uint32_t d = kLightSubpathDim;
+                const float u_sel = counter_u01(key, d++);
+                const float upx = counter_u01(key, d++), upy = counter_u01(key, d++);
+                const float udx = counter_u01(key, d++), udy = counter_u01(key, d++);
+                uint32_t li;
+                float sel;
+                light_select(P.sc, u_sel, li, sel);
+                const LightView L = load_light(P.sc, li);
+                f3 o, dir, nl;
+                float pdf_pos, pdf_dir;
+                bool ok = true;
+                if (L.kind == AR_LIGHT_POINT) {
+                    dir = uniform_sphere(udx, udy);
+                    o = L.pos;
+                    pdf_pos = 1.0f;
+                    pdf_dir = 1.0f / (4.0f * kPi);
+                    nl = dir;
+                } else {
+                    o = (L.pos + L.e1 * upx) + L.e2 * upy;
+                    const f3 local = cosine_hemisphere(udx, udy);
+                    const Onb f = onb_from_normal(L.n);
+                    dir = to_world(f, local);
+                    pdf_pos = 1.0f / L.area;
+                    pdf_dir = local.z * kInvPi;
+                    nl = L.n;
+                    ok = pdf_dir > 0.f;
+                }
+                if (ok) {
+                    r = Ray{o, normalize(dir), 1e-4f, FLT_MAX};
+                    const float pp = pdf_pos * sel;
+                    store_vtx(P, 1, 0, si, o, nl, L.inten / pp, pp, kTypeLight, L.kind == AR_LIGHT_POINT, li);
+                    P.nv[P.nsamples + si] = 1;
+                    f3 thr = L.inten / (pp * pdf_dir);
+                    thr = thr * fabsf(dot(nl, r.d));
+                    P.thr[q] = make_float4(thr.x, thr.y, thr.z, pdf_dir);
+                    P.dim[q] = d;
+                } else {
+                    P.nv[P.nsamples + si] = 0;
+                    live = false;
+                }
+            } else {
+                P.nv[P.nsamples + si] = 0;
+                live = false;
+            }
+            if (P.max_depth == 0) live = false;
+        }
+        const uint32_t slot = warp_alloc(&P.counts[0], live);
+        if (!live) continue;
+        P.ray_o[0][slot] = make_float4(r.o.x, r.o.y, r.o.z, r.tmin);
+        P.ray_d[0][slot] = make_float4(r.d.x, r.d.y, r.d.z, r.tmax);
+        P.qpath[0][slot] = q;
+    }
+}
+
+__global__ void __launch_bounds__(128) k_bd_extend(BdParams P, uint32_t depth, int* err) {
+    const uint32_t n = P.counts[depth];
+    const int b = depth & 1;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const float4 a = P.ray_o[b][j], d = P.ray_d[b][j];
+        HitRec h;
+        traverse<false>(P.sc, Ray{mk(a.x, a.y, a.z), mk(d.x, d.y, d.z), a.w, d.w}, h, err);
+        P.hit[j] = make_float4(h.t, h.u, h.v, __uint_as_float(h.slot));
+        P.hit_inst[j] = h.inst;
+    }
+}
+
+// One bounce of both subpaths (:368-434, :498-556).
+__global__ void __launch_bounds__(256) k_bd_vertex(BdParams P, uint32_t depth) {
+    const uint32_t n = P.counts[depth];
+    const int b = depth & 1;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t j = base + threadIdx.x;
+        bool cont = false;
+        uint32_t q = 0;
+        f3 no, nd;
+        if (j < n) {
+            q = P.qpath[b][j];
+            const uint32_t si = q >> 1, sub = q & 1u;
+            const float4 h = P.hit[j];
+            const uint32_t slot = __float_as_uint(h.w);
+            if (slot != kInvalid) {
+                const float4 ro4 = P.ray_o[b][j], rd4 = P.ray_d[b][j];
+                const f3 ro = mk(ro4.x, ro4.y, ro4.z), rd = mk(rd4.x, rd4.y, rd4.z);
+                const Shade s = make_shade(P.sc, ro, rd, h.x, h.y, h.z, slot, P.hit_inst[j]);
+                const MatView m = load_mat(P.sc, s.mat);
+                const float4 t4 = P.thr[q];
+                f3 thr = mk(t4.x, t4.y, t4.z);
+                const uint32_t k = P.nv[sub * P.nsamples + si];  // index of the new vertex
+                const size_t pi = vidx(P, sub, k - 1, si);
+                const float4 pa = P.va[pi], pb = P.vb[pi];
+                const f3 prev_p = mk(pa.x, pa.y, pa.z), prev_n = mk(pb.x, pb.y, pb.z);
+                const float pdf_fwd = pdf_sa_to_area(t4.w, prev_p, s.p, s.n);
+                store_vtx(P, sub, k, si, s.p, s.n, thr, pdf_fwd, kTypeSurface, false, s.mat);
+                P.nv[sub * P.nsamples + si] = uint8_t(k + 1);
+                const uint64_t g = P.sample_begin + si;
+                const uint32_t npix = P.width * P.height;
+                const uint64_t key = counter_key(P.seed, uint32_t(g % npix), uint32_t(g / npix));
+                uint32_t d = P.dim[q];
+                const f3 wo_l = to_local(s.onb, -rd);
+                d++;  // u_sel (unused by these BSDFs)
+                const float ux = counter_u01(key, d++), uy = counter_u01(key, d++);
+                f3 wi, f;
+                float pdf;
+                if (bsdf_sample(m, wo_l, ux, uy, wi, pdf, f) && pdf != 0.f && !is_zero(f)) {
+                    thr = thr * ((f * fabsf(wi.z)) / pdf);
+                    const float pdf_rev_dir = bsdf_pdf(m, wo_l, wi);
+                    P.vb[pi].w = pdf_sa_to_area(pdf_rev_dir, s.p, prev_p, prev_n);
+                    bool alive = true;
+                    if (depth + 1 >= P.rr_depth) {
+                        const float survival = fminf(max3(thr), 0.95f);
+                        if (counter_u01(key, d++) > survival || survival <= 0.f) alive = false;
+                        else thr = thr / survival;
+                    }
+                    if (alive && depth + 1 < P.max_depth) {
+                        const f3 wi_w = to_world(s.onb, wi);
+                        no = s.p + (s.n * 1e-4f) * signum(dot(wi_w, s.n));
+                        nd = normalize(wi_w);
+                        P.thr[q] = make_float4(thr.x, thr.y, thr.z, pdf);
+                        P.dim[q] = d;
+                        cont = true;
+                    }
+                }
+            }
+        }
+        const uint32_t rs = warp_alloc(&P.counts[depth + 1], cont);
+        if (cont) {
+            P.ray_o[b ^ 1][rs] = make_float4(no.x, no.y, no.z, 1e-4f);
+            P.ray_d[b ^ 1][rs] = make_float4(nd.x, nd.y, nd.z, FLT_MAX);
+            P.qpath[b ^ 1][rs] = q;
+        }
+    }
+}
+
+// connect_bdpt for s >= 2 (:782-1044) + the t == 0 extension.  Emits a shadow
+// ray with the MIS-weighted contribution, or deposits directly when t == 0.
+__device__ void connect_general(const BdParams& P, uint32_t si, uint32_t S, uint32_t T, uint32_t s, uint32_t t,
+                                uint32_t pix) {
+    const Vtx z = load_vtx(P, 0, s - 1, si);
+    const Vtx zp = load_vtx(P, 0, s - 2, si);
+    if (t == 0) {
+        const MatView mz = load_mat(P.sc, z.index);
+        if (mz.emitter < 0 || !light_enabled(P.sc)) return;
+        const LightView lt = load_light(P.sc, uint32_t(mz.emitter));
+        const f3 wo = normalize(zp.p - z.p);
+        if (dot(lt.n, wo) <= 0.f) return;
+        const f3 c = z.thr * lt.inten;
+        if (max3(c) <= 0.f) return;
+        const float pdf_cc = light_pmf_of(P.sc, uint32_t(mz.emitter)) / lt.area;
+        const float w = mis_weight(P, si, S, T, s, 0, pdf_cc, 0.f);
+        film_add(P, pix, (c * w) * P.inv_spp);
+        return;
+    }
+    const Vtx y = load_vtx(P, 1, t - 1, si);
+    if (y.type == kTypeSurface && y.delta) return;
+    const f3 d = y.p - z.p;
+    const float d2 = dot(d, d);
+    if (d2 < 1e-10f) return;
+    const float dist = sqrtf(d2);
+    const f3 wi_z = d / dist;
+    const f3 wi_y = -wi_z;
+    const f3 so = z.p + (z.n * 1e-4f) * signum(dot(wi_z, z.n));
+    const f3 st = y.p + (y.n * 1e-4f) * signum(dot(wi_y, y.n));
+    const f3 sd = st - so;
+    const float sdist = length(sd);
+    if (sdist < 1e-6f) return;
+    const Onb oz = onb_from_normal(z.n);
+    const MatView mz = load_mat(P.sc, z.index);
+    const f3 wo_z = normalize(zp.p - z.p);
+    const f3 wo_zl = to_local(oz, wo_z);
+    const f3 f_z = bsdf_eval(mz, to_local(oz, wi_z), wo_zl);
+    if (is_zero(f_z)) return;
+    f3 f_y = mk(1.f, 1.f, 1.f);
+    Onb oy;
+    MatView my;
+    f3 wo_yl = mk(0.f, 0.f, 0.f);
+    if (t != 1) {
+        oy = onb_from_normal(y.n);
+        my = load_mat(P.sc, y.index);
+        const Vtx yp = load_vtx(P, 1, t - 2, si);
+        wo_yl = to_local(oy, normalize(yp.p - y.p));
+        f_y = bsdf_eval(my, to_local(oy, wi_y), wo_yl);
+    }
+    if (is_zero(f_y)) return;
+    const float g = geometry_term(z.p, z.n, y.p, y.n);
+    f3 c;
+    if (t == 1) {
+        const LightView L = load_light(P.sc, y.index);
+        if (L.kind == AR_LIGHT_POINT) {
+            // :951-967 — re-sample the point light toward z
+            f3 lwi, lrad;
+            float ldist, lpdf;
+            if (!light_sample(L, z.p, 0.f, 0.f, lwi, ldist, lrad, lpdf)) return;
+            const f3 f_direct = bsdf_eval(mz, to_local(oz, lwi), wo_zl);
+            c = ((z.thr * f_direct) * fabsf(dot(z.n, lwi))) * lrad;
+        } else {
+            if (dot(y.n, wi_y) <= 0.f) return;
+            c = ((z.thr * f_z) * g) * y.thr;
+        }
+    } else {
+        c = (((z.thr * f_z) * g) * f_y) * y.thr;
+    }
+    if (max3(c) <= 0.f) return;
+    float pdf_cc;
+    if (t == 1) {
+        const LightView L = load_light(P.sc, y.index);
+        pdf_cc = pdf_sa_to_area(light_pdf_emission_dir(L, normalize(z.p - y.p)), y.p, z.p, z.n);
+    } else {
+        const f3 wiy = normalize(z.p - y.p);
+        pdf_cc = pdf_sa_to_area(bsdf_pdf(my, to_local(oy, wiy), wo_yl), y.p, z.p, z.n);
+    }
+    const float pdf_cl = pdf_sa_to_area(bsdf_pdf(mz, to_local(oz, normalize(y.p - z.p)), wo_zl), z.p, y.p, y.n);
+    const float w = mis_weight(P, si, S, T, s, t, pdf_cc, pdf_cl);
+    push_shadow(P, so, normalize(sd / sdist), sdist * (1.0f - 1e-4f), c * w, pix);
+}
+
+// connect_bdpt_s1 (:1051-1155): light tracing to the pinhole, splatted.
+__device__ void connect_s1(const BdParams& P, uint32_t si, uint32_t S, uint32_t T, uint32_t t) {
+    const Vtx y = load_vtx(P, 1, t - 1, si);
+    if (y.type == kTypeSurface && y.delta) return;
+    // PinholeCamera::sample_we (src/cameras.rs:175-240)
+    const f3 co = ld3(P.cam.o);
+    const f3 to_cam0 = co - y.p;
+    const float d2 = dot(to_cam0, to_cam0);
+    const float dist = sqrtf(d2);
+    if (dist < 1e-6f) return;
+    const f3 wi = to_cam0 / dist;
+    const f3 dir = -wi;
+    const float ct = dot(dir, ld3(P.cam.fwd));
+    if (ct <= 1e-6f) return;
+    const f3 ds = dir / ct;
+    const float u = dot(ds, ld3(P.cam.right)) / P.cam.vw + 0.5f;
+    const float v = dot(ds, ld3(P.cam.up)) / P.cam.vh + 0.5f;
+    if (u < 0.f || u > 1.f || v < 0.f || v > 1.f) return;
+    const float px = u * float(P.width);
+    const float py = (1.0f - v) * float(P.height);
+    if (px < 0.f || px >= float(P.width) || py < 0.f || py >= float(P.height)) return;
+    const float c2 = ct * ct, c4 = c2 * c2;
+    const float we = 1.0f / (P.cam.area * c4);
+    const Onb oy = onb_from_normal(y.n);
+    const MatView my = load_mat(P.sc, y.index);
+    const Vtx yp = load_vtx(P, 1, t - 2, si);
+    const f3 wo_yl = to_local(oy, normalize(yp.p - y.p));
+    const f3 f_y = bsdf_eval(my, to_local(oy, wi), wo_yl);
+    if (is_zero(f_y)) return;
+    const float gf = fabsf(dot(y.n, wi)) / (dist * dist);
+    const f3 c = ((y.thr * f_y) * gf) * we;
+    if (max3(c) <= 0.f) return;
+    const Vtx z0 = load_vtx(P, 0, 0, si);
+    const float pdf_cl = pdf_sa_to_area(bsdf_pdf(my, to_local(oy, wi), wo_yl), y.p, co, z0.n);
+    const float w = mis_weight(P, si, S, T, 1, t, 0.f, pdf_cl);
+    const uint32_t ix = min(uint32_t(px), P.width - 1), iy = min(uint32_t(py), P.height - 1);
+    const f3 o = y.p + (y.n * 1e-4f) * signum(dot(wi, y.n));
+    push_shadow(P, o, normalize(wi), dist * (1.0f - 1e-4f), c * w, iy * P.width + ix);
+}
+
+__global__ void __launch_bounds__(128) k_bd_connect(BdParams P) {
+    const uint32_t npix = P.width * P.height;
+    for (uint32_t si = blockIdx.x * blockDim.x + threadIdx.x; si < P.nsamples; si += gridDim.x * blockDim.x) {
+        const uint32_t S = P.nv[si], T = P.nv[P.nsamples + si];
+        const uint32_t pix = uint32_t((P.sample_begin + si) % npix);
+        const uint32_t limit = P.max_depth + 2;
+        for (uint32_t t = 0; t <= T; ++t)
+            for (uint32_t s = 1; s <= S; ++s) {
+                if (s + t < 2 || s + t > limit) continue;
+                if (s == 1) {
+                    if (t >= 2) connect_s1(P, si, S, T, t);
+                    continue;
+                }
+                connect_general(P, si, S, T, s, t, pix);
+            }
+    }
+}
+
+__global__ void __launch_bounds__(128) k_bd_shadow(BdParams P, int* err) {
+    const uint32_t n = min(P.counts[64], P.sh_cap);
+    for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
+        const float4 a = P.sh_o[m], d = P.sh_d[m];
+        HitRec h;
+        traverse<true>(P.sc, Ray{mk(a.x, a.y, a.z), mk(d.x, d.y, d.z), 0.f, d.w}, h, err);
+        if (h.slot == kInvalid) {
+            const float4 c = P.sh_c[m];
+            film_add(P, __float_as_uint(c.w), mk(c.x, c.y, c.z) * P.inv_spp);
+        }
+    }
+}
+
+__global__ void k_bd_count(const uint32_t* counts, uint32_t max_depth, unsigned long long* stats, int* err) {
+    if (threadIdx.x == 0) {
+        unsigned long long ext = 0;
+        for (uint32_t d = 0; d < max_depth; ++d) ext += counts[d];
+        stats[0] += counts[0];
+        stats[1] += ext;
+        stats[2] += counts[64];
+        if (counts[65]) atomicExch(err, 4);
+    }
+}
+
+template <class T>
+T* carve(char*& cur, size_t n) {
+    cur = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(cur) + 255) & ~uintptr_t(255));
+    T* p = reinterpret_cast<T*>(cur);
+    cur += n * sizeof(T);
+    return p;
+}
+
+}  // namespace
+
+void render_bdpt_film(ar_context* ctx, const ar_scene* sc, const CameraDev& cam, const ar_integrator_cfg& cfg,
+                      uint32_t w, uint32_t h, void* film) {
+    AR_REQUIRE(cfg.max_depth <= 62, AR_ERR_INVALID_ARGUMENT, "max_depth must be <= 62");
+    const uint64_t total = uint64_t(w) * h * cfg.spp;
+    const uint32_t maxv = cfg.max_depth + 1;
+    // Worst-case connections per sample: (s, t) pairs with 1 <= s, t <= maxv, s + t <= max_depth + 2.
+    uint32_t max_pairs = 0;
+    for (uint32_t t = 0; t <= maxv; ++t)
+        for (uint32_t s = 1; s <= maxv; ++s)
+            if (s + t >= 2 && s + t <= cfg.max_depth + 2) max_pairs++;
+    const size_t per_sample = size_t(2) * maxv * 48 + 2 + 2 * (16 + 4) + 2 * 2 * (32 + 4) + 2 * 20 +
+                              size_t(max_pairs) * 48;
+    const size_t budget = size_t(3) << 30;
+    const uint32_t chunk = uint32_t(std::max<uint64_t>(1024, std::min<uint64_t>(total, budget / per_sample)));
+    ctx->work.ensure(per_sample * chunk + 64 * 1024);
+    char* cur = ctx->work.buf.as<char>();
+    BdParams P{};
+    P.sc = sc->view;
+    P.cam = cam;
+    P.width = w;
+    P.height = h;
+    P.spp = cfg.spp;
+    P.max_depth = cfg.max_depth;
+    P.rr_depth = cfg.rr_depth;
+    P.mis_mode = cfg.mis_mode;
+    P.mis_beta = cfg.mis_beta;
+    P.film64 = cfg.film_precision == AR_FILM_F64 ? 1u : 0u;
+    P.seed = cfg.seed;
+    P.maxv = maxv;
+    P.inv_spp = 1.0f / float(cfg.spp);
+    P.film = film;
+    const size_t nvtx = size_t(2) * maxv * chunk;
+    P.va = carve<float4>(cur, nvtx);
+    P.vb = carve<float4>(cur, nvtx);
+    P.vc = carve<float4>(cur, nvtx);
+    P.nv = carve<uint8_t>(cur, 2 * size_t(chunk));
+    P.thr = carve<float4>(cur, 2 * size_t(chunk));
+    P.dim = carve<uint32_t>(cur, 2 * size_t(chunk));
+    for (int b = 0; b < 2; ++b) {
+        P.ray_o[b] = carve<float4>(cur, 2 * size_t(chunk));
+        P.ray_d[b] = carve<float4>(cur, 2 * size_t(chunk));
+        P.qpath[b] = carve<uint32_t>(cur, 2 * size_t(chunk));
+    }
+    P.hit = carve<float4>(cur, 2 * size_t(chunk));
+    P.hit_inst = carve<uint32_t>(cur, 2 * size_t(chunk));
+    P.sh_cap = uint32_t(std::min<uint64_t>(uint64_t(max_pairs) * chunk, 0xFFFFFFF0ull));
+    P.sh_o = carve<float4>(cur, P.sh_cap);
+    P.sh_d = carve<float4>(cur, P.sh_cap);
+    P.sh_c = carve<float4>(cur, P.sh_cap);
+    P.counts = carve<uint32_t>(cur, 128);
+    const size_t film_bytes = size_t(w) * h * 3 * (P.film64 ? sizeof(double) : sizeof(float));
+    AR_CUDA(cudaMemsetAsync(film, 0, film_bytes, ctx->stream));
+    AR_CUDA(cudaMemsetAsync(ctx->stats_d.ptr, 0, 8 * sizeof(uint64_t), ctx->stream));
+    int* err = ctx->err_flag.as<int>();
+    const int wide = ctx->num_sms * 8;
+    uint64_t chunks = 0;
+    for (uint64_t begin = 0; begin < total; begin += chunk, ++chunks) {
+        P.sample_begin = begin;
+        P.nsamples = uint32_t(std::min<uint64_t>(chunk, total - begin));
+        AR_CUDA(cudaMemsetAsync(P.counts, 0, 128 * sizeof(uint32_t), ctx->stream));
+        {
+            KernelScope ks(ctx->prof, ctx->stream, "bdpt_generate");
+            k_bd_generate<<<std::max(1, int(std::min<uint64_t>((2ull * P.nsamples + 255) / 256, wide))), 256, 0,
+                            ctx->stream>>>(P);
+        }
+        for (uint32_t d = 0; d < cfg.max_depth; ++d) {
+            {
+                KernelScope ks(ctx->prof, ctx->stream, "bdpt_extend");
+                k_bd_extend<<<ctx->num_sms * 16, 128, 0, ctx->stream>>>(P, d, err);
+            }
+            {
+                KernelScope ks(ctx->prof, ctx->stream, "bdpt_vertex");
+                k_bd_vertex<<<wide, 256, 0, ctx->stream>>>(P, d);
+            }
+        }
+        {
+            KernelScope ks(ctx->prof, ctx->stream, "bdpt_connect");
+            k_bd_connect<<<std::max(1, int(std::min<uint64_t>((P.nsamples + 127) / 128, ctx->num_sms * 16))), 128, 0,
+                           ctx->stream>>>(P);
+        }
+        {
+            KernelScope ks(ctx->prof, ctx->stream, "bdpt_shadow");
+            k_bd_shadow<<<ctx->num_sms * 16, 128, 0, ctx->stream>>>(P, err);
+        }
+        k_bd_count<<<1, 32, 0, ctx->stream>>>(P.counts, cfg.max_depth, ctx->stats_d.as<unsigned long long>(), err);
+        AR_CUDA(cudaGetLastError());
+    }
+    AR_CUDA(cudaMemcpyAsync(ctx->stats_h, ctx->stats_d.ptr, 8 * sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    ctx->stats_pending = true;
+    ctx->last_stats.path_samples = total;
+    ctx->last_stats.extend_launches = chunks * cfg.max_depth;
+    ctx->last_stats.shadow_launches = chunks;
+}
+
+}  // namespace ar

@@ -58,6 +58,8 @@ int ar_context_create(int device, ar_context** out) {
         AR_CUDA(cudaMemset(ctx->err_flag.ptr, 0, 64));
         ctx->stats_d.alloc(8 * sizeof(uint64_t));
         AR_CUDA(cudaMemset(ctx->stats_d.ptr, 0, 8 * sizeof(uint64_t)));
+        AR_CUDA(cudaMallocHost(&ctx->stats_h, 8 * sizeof(uint64_t)));
+        std::memset(ctx->stats_h, 0, 8 * sizeof(uint64_t));
         *out = ctx.release();
     });
 }
@@ -68,6 +70,7 @@ int ar_context_destroy(ar_context* ctx) {
         cudaSetDevice(ctx->device);
         if (ctx->stream) cudaStreamSynchronize(ctx->stream);
         if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+        if (ctx->stats_h) cudaFreeHost(ctx->stats_h);
         delete ctx;
     });
 }

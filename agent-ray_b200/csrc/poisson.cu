@@ -214,9 +214,8 @@ void poisson_reconstruct(ar_context* ctx, const ar_integrator_cfg& cfg, uint32_t
     const int grid = std::max(1, std::min(int((n + 255) / 256), ctx->num_sms * 8));
     cudaStream_t st = ctx->stream;
     if (cfg.poisson_solver == AR_POISSON_SOR) {
-        ar::DevBuf tmp;
-        tmp.alloc(2 * 3 * n * sizeof(float));
-        float* rhs = tmp.as<float>();
+        ctx->solver.ensure(2 * 3 * n * sizeof(float));
+        float* rhs = ctx->solver.buf.as<float>();
         float* img = rhs + 3 * n;
         k_rhs<<<grid, 256, 0, st>>>(w, h, primal, gx, gy, cfg.alpha, rhs, img);
         for (uint32_t it = 0; it < cfg.poisson_iterations; ++it)
@@ -224,7 +223,6 @@ void poisson_reconstruct(ar_context* ctx, const ar_integrator_cfg& cfg, uint32_t
                 k_sor_half<<<grid, 256, 0, st>>>(w, h, parity, rhs, img, cfg.alpha, cfg.sor_omega);
         k_clamp<<<grid, 256, 0, st>>>(3 * n, img, out);
         AR_CUDA(cudaGetLastError());
-        AR_CUDA(cudaStreamSynchronize(st));
         if (rel_residual) *rel_residual = -1.0;
         return;
     }
@@ -233,9 +231,8 @@ void poisson_reconstruct(ar_context* ctx, const ar_integrator_cfg& cfg, uint32_t
     const double tol = cfg.poisson_tolerance > 0 ? cfg.poisson_tolerance : 1e-6;
     const uint32_t max_total = cfg.poisson_iterations ? cfg.poisson_iterations : 1000;
     const uint32_t inner = 32;
-    ar::DevBuf tmp;
-    tmp.alloc(3 * n * (2 * sizeof(double) + 4 * sizeof(float)) + 16 * sizeof(double) + 1024);
-    double* b = tmp.as<double>();
+    ctx->solver.ensure(3 * n * (2 * sizeof(double) + 4 * sizeof(float)) + 16 * sizeof(double) + 1024);
+    double* b = ctx->solver.buf.as<double>();
     double* x = b + 3 * n;
     float* r = reinterpret_cast<float*>(x + 3 * n);
     float* p = r + 3 * n;

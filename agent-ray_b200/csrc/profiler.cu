@@ -99,7 +99,15 @@ int ar_profile_read(ar_context* ctx, char* names, uint32_t capacity, double* ms,
 int ar_get_render_stats(const ar_context* ctx, ar_render_stats* out) {
     return guarded([&] {
         AR_REQUIRE(ctx && out, AR_ERR_INVALID_ARGUMENT, "null argument");
-        *out = ctx->last_stats;
+        ar_context* c = const_cast<ar_context*>(ctx);
+        if (c->stats_pending) {
+            AR_CUDA(cudaStreamSynchronize(c->stream));
+            c->last_stats.paths = c->stats_h[0];
+            c->last_stats.extend_rays = c->stats_h[1];
+            c->last_stats.shadow_rays = c->stats_h[2];
+            c->stats_pending = false;
+        }
+        *out = c->last_stats;
     });
 }
 

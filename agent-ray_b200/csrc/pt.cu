@@ -401,13 +401,11 @@ void render_pt_films(ar_context* ctx, const ar_scene* sc, const CameraDev& cam, 
         k_count<<<1, 64, 0, ctx->stream>>>(P.st.counts, cfg.max_depth, ctx->stats_d.as<unsigned long long>());
         AR_CUDA(cudaGetLastError());
     }
-    uint64_t st[8];
-    AR_CUDA(cudaMemcpyAsync(st, ctx->stats_d.ptr, sizeof(st), cudaMemcpyDeviceToHost, ctx->stream));
-    AR_CUDA(cudaStreamSynchronize(ctx->stream));
+    // Counters land in pinned memory; ar_get_render_stats reads them after a sync.
+    AR_CUDA(cudaMemcpyAsync(ctx->stats_h, ctx->stats_d.ptr, 8 * sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    ctx->stats_pending = true;
     ctx->last_stats.path_samples = total;
-    ctx->last_stats.paths = st[0];
-    ctx->last_stats.extend_rays = st[1];
-    ctx->last_stats.shadow_rays = st[2];
     ctx->last_stats.extend_launches = chunks * cfg.max_depth;
     ctx->last_stats.shadow_launches = chunks * cfg.max_depth;
 }

@@ -6,6 +6,8 @@
 
 namespace ar {
 
+void check_device_flag(ar_context* ctx);
+
 namespace {
 
 struct V {
@@ -76,37 +78,30 @@ void render(ar_context* ctx, const ar_scene* sc, const ar_camera_desc& camd, con
     const bool f64 = cfg.film_precision == AR_FILM_F64;
     const size_t film_bytes = count * (f64 ? sizeof(double) : sizeof(float));
     const int nfilms = cfg.integrator == AR_INTEGRATOR_GDPT ? 3 : 1;
-    DevBuf films;
-    films.alloc(film_bytes * nfilms + count * sizeof(float) * (nfilms + 1));
-    float* dev_out_tmp = reinterpret_cast<float*>(films.as<char>() + film_bytes * nfilms);
+    Workspace& films = ctx->films;
+    films.ensure(film_bytes * nfilms + count * sizeof(float) * (nfilms + 1));
+    float* dev_out_tmp = reinterpret_cast<float*>(films.buf.as<char>() + film_bytes * nfilms);
     float* dev_out = out_on_device ? out : dev_out_tmp;
     if (cfg.integrator == AR_INTEGRATOR_PT) {
-        render_pt_films(ctx, sc, cam, cfg, w, h, false, films.ptr);
-        film_to_f32(ctx, films.ptr, f64, count, dev_out);
+        render_pt_films(ctx, sc, cam, cfg, w, h, false, films.buf.ptr);
+        film_to_f32(ctx, films.buf.ptr, f64, count, dev_out);
     } else if (cfg.integrator == AR_INTEGRATOR_BDPT) {
-        render_bdpt_film(ctx, sc, cam, cfg, w, h, films.ptr);
-        film_to_f32(ctx, films.ptr, f64, count, dev_out);
+        render_bdpt_film(ctx, sc, cam, cfg, w, h, films.buf.ptr);
+        film_to_f32(ctx, films.buf.ptr, f64, count, dev_out);
     } else {
-        render_pt_films(ctx, sc, cam, cfg, w, h, true, films.ptr);
+        render_pt_films(ctx, sc, cam, cfg, w, h, true, films.buf.ptr);
         float* f32films = dev_out_tmp + count;  // primal, dx, dy as f32
         for (int f = 0; f < 3; ++f)
-            film_to_f32(ctx, films.as<char>() + f * film_bytes, f64, count, f32films + f * count);
+            film_to_f32(ctx, films.buf.as<char>() + f * film_bytes, f64, count, f32films + f * count);
         poisson_reconstruct(ctx, cfg, w, h, f32films, f32films + count, f32films + 2 * count, dev_out, nullptr);
     }
-    if (!out_on_device)
+    // Device output stays asynchronous on the context stream (errors surface at
+    // the next ar_context_synchronize); host output synchronises here.
+    if (!out_on_device) {
         AR_CUDA(cudaMemcpyAsync(out, dev_out, count * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
-    AR_CUDA(cudaStreamSynchronize(ctx->stream));
-    int flag = 0;
-    AR_CUDA(cudaMemcpy(&flag, ctx->err_flag.ptr, sizeof(int), cudaMemcpyDeviceToHost));
-    if (flag) {
-        AR_CUDA(cudaMemset(ctx->err_flag.ptr, 0, sizeof(int)));
-        throw ArError{AR_ERR_INTERNAL, "traversal stack overflow"};
+        check_device_flag(ctx);
     }
 }
 
-void render_bdpt_film(ar_context*, const ar_scene*, const CameraDev&, const ar_integrator_cfg&, uint32_t, uint32_t,
-                      void*) {
-    throw ArError{AR_ERR_UNSUPPORTED, "BDPT is not built yet"};
-}
 
 }  // namespace ar

@@ -220,7 +220,11 @@ def run_ours(args, rank, local, world):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     peaks, peak_kind = load_peaks()
     ctx = agentray.Context(local)
-    stream = torch.cuda.current_stream()
+    # A dedicated stream: the library launches on it, and every timing event is
+    # recorded on it (torch's legacy default stream has handle 0, which the C ABI
+    # reads as "use the context's own stream").
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -256,9 +260,10 @@ def run_ours(args, rank, local, world):
             pt.render(scene, cam, W, H, out=out)
             e1.record(stream)
             step_ms.append((e0, e1))
-            st = ctx.render_stats()
-            launches += st["extend_launches"] * 3 + 2 * (st["extend_launches"] // cfg.max_depth)
         torch.cuda.synchronize()
+    st = ctx.render_stats()
+    # per render: generate + (extend, shade, shadow) x depth + counter fold, per chunk
+    launches = args.steps * (st["extend_launches"] * 3 + 2 * (st["extend_launches"] // cfg.max_depth))
     barrier()
     ctx.profile(False)
     prof = ctx.profile_read()
@@ -337,6 +342,7 @@ def run_bvh(args, rank, world, ctx, torch, flush, barrier, dist, peaks, peak_kin
     ot_d = torch.from_numpy(ot).cuda()
     dt_d = torch.from_numpy(dt).cuda()
     stream = torch.cuda.current_stream()
+    assert stream.cuda_stream != 0
     for _ in range(max(3, args.warmup)):
         scene.trace_closest(ot_d, dt_d)
     torch.cuda.synchronize()

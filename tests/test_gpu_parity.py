@@ -200,3 +200,26 @@ def test_gdpt_same_stream_matches_oracle(ctx):
     assert abs(gpu.mean() - ref.mean()) / ref.mean() < 1e-2
     close = np.abs(gpu - ref) <= 2e-2 * np.maximum(1.0, np.abs(ref))
     assert close.all(axis=2).mean() >= 0.95
+
+
+@pytest.mark.parametrize("point_light", [True, False])
+def test_bdpt_same_stream_matches_oracle(ctx, point_light):
+    sc, cam = S.cornell_box(1, point_light=point_light)
+    cfg = integrator_cfg(A.INTEGRATOR_BDPT, spp=8, max_depth=6, rr_depth=3, seed=4)
+    w = h = 48
+    gpu = _render_gpu(ctx, sc, cam, cfg, w, h)
+    ref = O.OracleScene(sc).render(cam, cfg, w, h, sampler=O.SAMPLER_COUNTER)
+    assert abs(gpu.mean() - ref.mean()) / ref.mean() < 1e-2
+    close = np.abs(gpu - ref) <= 1e-2 * np.maximum(1.0, np.abs(ref))
+    assert close.all(axis=2).mean() >= 0.95, close.all(axis=2).mean()
+
+
+def test_bdpt_statistically_equal_to_independent_oracle(ctx):
+    sc, cam = S.cornell_box(1)
+    w = h = 32
+    osc = O.OracleScene(sc)
+    g = np.stack([_render_gpu(ctx, sc, cam, integrator_cfg(A.INTEGRATOR_BDPT, spp=16, max_depth=6, seed=400 + k),
+                              w, h) for k in range(8)])
+    r = np.stack([osc.render(cam, integrator_cfg(A.INTEGRATOR_BDPT, spp=16, max_depth=6, seed=500 + k), w, h,
+                             sampler=O.SAMPLER_COUNTER) for k in range(8)])
+    assert welch_fail_fraction(g, r) < 0.01

@@ -25,7 +25,7 @@ from .scene_data import Camera, Light, Material, Mesh, Object, SceneData, integr
 
 __all__ = ["Context", "Scene", "Camera", "Film", "PathTracer", "PathTracerConfig", "BidirectionalPathTracer",
            "BdptConfig", "GradientDomainPathTracer", "GdptConfig", "SceneData", "Mesh", "Object", "Material",
-           "Light", "AgentRayError", "integrator_cfg", "lib"]
+           "Light", "AgentRayError", "integrator_cfg", "lib", "Server", "poisson_reconstruct"]
 
 
 class Context:
@@ -240,6 +240,75 @@ class BidirectionalPathTracer(_Integrator):
 
 class GradientDomainPathTracer(_Integrator):
     kind = A.INTEGRATOR_GDPT
+
+
+class Server:
+    """Render server (ar_server): continuously batches submitted jobs into
+    shared wavefront kernels on one GPU.  submit() returns a job id at once;
+    the image lands in the job's host buffer before its status becomes DONE."""
+
+    STATUS = {A.JOB_PENDING: "pending", A.JOB_RUNNING: "running", A.JOB_DONE: "done", A.JOB_REJECTED: "rejected",
+              A.JOB_CANCELLED: "cancelled", A.JOB_FAILED: "failed"}
+
+    def __init__(self, ctx: Context, film_budget_bytes=0, path_capacity=0, bdpt_batch_samples=0, bdpt_max_depth=0,
+                 max_active_jobs=0):
+        self.ctx = ctx
+        self.handle = C.c_void_p()
+        o = A.ServerOpts(film_budget_bytes, path_capacity, bdpt_batch_samples, bdpt_max_depth, max_active_jobs)
+        check(lib().ar_server_create(ctx.handle, C.byref(o), C.byref(self.handle)))
+        self.outputs = {}
+        self._keep = {}
+
+    def submit(self, scene: Scene, camera: Camera, integrator, width, height):
+        out = np.empty(width * height * 3, np.float32)
+        cam = camera.desc()
+        cfg = integrator.cfg()
+        jid = C.c_uint64()
+        check(lib().ar_job_submit(self.handle, scene.handle, C.byref(cam), C.byref(cfg), width, height,
+                                  out.ctypes.data, C.byref(jid)))
+        self.outputs[jid.value] = out.reshape(height, width, 3)
+        self._keep[jid.value] = scene
+        return jid.value
+
+    @staticmethod
+    def _info(i):
+        return {"status": Server.STATUS[i.status], "error": i.error, "submit_ms": i.submit_ms,
+                "admit_ms": i.admit_ms, "done_ms": i.done_ms, "path_samples": i.path_samples}
+
+    def poll(self, job_id):
+        i = A.JobInfo()
+        check(lib().ar_job_poll(self.handle, job_id, C.byref(i)))
+        return self._info(i)
+
+    def wait(self, job_id, timeout_ms=600_000.0):
+        i = A.JobInfo()
+        check(lib().ar_job_wait(self.handle, job_id, timeout_ms, C.byref(i)))
+        return self._info(i)
+
+    def cancel(self, job_id):
+        check(lib().ar_job_cancel(self.handle, job_id))
+
+    def result(self, job_id):
+        return self.outputs[job_id]
+
+    def stats(self):
+        s = A.ServerStats()
+        check(lib().ar_server_get_stats(self.handle, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in A.ServerStats._fields_}
+
+    def now_ms(self):
+        return lib().ar_server_now_ms(self.handle)
+
+    def close(self):
+        if self.handle:
+            check(lib().ar_server_destroy(self.handle))
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def poisson_reconstruct(ctx: Context, primal, grad_x, grad_y, alpha=0.2, solver=A.POISSON_SOR, iterations=200,

@@ -100,6 +100,26 @@ assert C.sizeof(MaterialDesc) == 40
 assert C.sizeof(LightDesc) == 56
 
 
+JOB_PENDING, JOB_RUNNING, JOB_DONE, JOB_REJECTED, JOB_CANCELLED, JOB_FAILED = range(6)
+
+
+class ServerOpts(C.Structure):
+    _fields_ = [("film_budget_bytes", C.c_uint64), ("path_capacity", u32), ("bdpt_batch_samples", u32),
+                ("bdpt_max_depth", u32), ("max_active_jobs", u32)]
+
+
+class JobInfo(C.Structure):
+    _fields_ = [("status", u32), ("error", C.c_int32), ("submit_ms", C.c_double), ("admit_ms", C.c_double),
+                ("done_ms", C.c_double), ("path_samples", C.c_uint64)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("jobs_submitted", C.c_uint64), ("jobs_done", C.c_uint64), ("jobs_rejected", C.c_uint64),
+                ("jobs_cancelled", C.c_uint64), ("jobs_failed", C.c_uint64), ("path_samples_done", C.c_uint64),
+                ("pt_ticks", C.c_uint64), ("bdpt_batches", C.c_uint64), ("film_bytes_in_use", C.c_uint64),
+                ("film_bytes_peak", C.c_uint64)]
+
+
 class RenderStats(C.Structure):
     _fields_ = [("path_samples", C.c_uint64), ("paths", C.c_uint64), ("extend_rays", C.c_uint64),
                 ("shadow_rays", C.c_uint64), ("extend_launches", C.c_uint64), ("shadow_launches", C.c_uint64)]

@@ -209,6 +209,67 @@ def room(seed=4, sphere_levels=(6, 6, 5, 4), n_boxes=500, point_lights=False):
     return sc, cam
 
 
+SERVED_TRIANGLES = [10_000, 19_307, 37_276, 71_969, 138_950, 268_270, 517_947, 1_000_000]
+
+
+def served_scene(k, seed=5):
+    """Scene k of the 8 served-stream scenes: triangle counts log-spaced from
+    10k to 1M (SERVED_TRIANGLES), built from a room box, icospheres and
+    instanced boxes, Lambertian/GGX 50/50, two quad lights.  Returns
+    (scene_data, camera)."""
+    target = SERVED_TRIANGLES[k]
+    rng = np.random.default_rng(seed * 100 + k)
+    sc = SceneData(A.LIGHT_DIST_POWER)
+    W, H, D = 10.0, 5.0, 10.0
+    walls = [((0, 0, 0), (0, 0, D), (W, 0, 0)), ((0, H, 0), (W, 0, 0), (0, 0, D)), ((0, 0, 0), (W, 0, 0), (0, H, 0)),
+             ((0, 0, D), (0, H, 0), (W, 0, 0)), ((0, 0, 0), (0, H, 0), (0, 0, D)), ((W, 0, 0), (0, 0, D), (0, H, 0))]
+    pos, idx = [], []
+    for i, (c, e1, e2) in enumerate(walls):
+        q = quad_mesh(c, e1, e2)
+        pos.append(q.positions)
+        idx.append(q.indices + 4 * i)
+    m = sc.add_mesh(Mesh(np.concatenate(pos), np.concatenate(idx)))
+    sc.add_object(Object(m, [sc.add_material(Material(A.MATERIAL_LAMBERTIAN, albedo=tuple(rng.uniform(0.2, 0.8, 3))))]))
+    remaining = target - 12 - 4
+    n_boxes = min(300, max(20, remaining // 200))
+    remaining -= 12 * n_boxes
+    sphere_meshes = {}
+    while remaining >= 20 * 4 ** 2:
+        lvl = max(l for l in range(2, 9) if 20 * 4 ** l <= remaining)
+        if lvl not in sphere_meshes:
+            sphere_meshes[lvl] = sc.add_mesh(icosphere(lvl))
+        r = float(rng.uniform(0.4, 1.2))
+        ctr = (rng.uniform(1.0, W - 1.0), r, rng.uniform(1.0, D - 1.0))
+        xf, inv = trs(ctr, None, (r, r, r))
+        sc.add_object(Object(sphere_meshes[lvl], [sc.add_material(random_material(rng))], xf, inv))
+        remaining -= 20 * 4 ** lvl
+    n_boxes += remaining // 12
+    cube = sc.add_mesh(unit_cube_mesh())
+    for _ in range(n_boxes):
+        s = rng.uniform(0.1, 0.5, 3)
+        t = (rng.uniform(0.3, W - 0.3), rng.uniform(0.2, H - 0.6), rng.uniform(0.3, D - 0.3))
+        xf, inv = trs(t, random_rotation(rng), s)
+        sc.add_object(Object(cube, [sc.add_material(random_material(rng))], xf, inv))
+    add_quad_light(sc, (2.5, 4.99, 4.5), (1.0, 0.0, 0.0), (0.0, 0.0, 1.0), (12.0, 12.0, 12.0))
+    add_quad_light(sc, (6.5, 4.99, 4.5), (1.0, 0.0, 0.0), (0.0, 0.0, 1.0), (10.0, 11.0, 12.0))
+    cam = Camera((5.0, 2.5, 9.6), (5.0, 1.8, 0.0), (0.0, 1.0, 0.0), 60.0, 1.0)
+    return sc, cam
+
+
+def served_stream(n_jobs=2000, seed=5, rate_hz=1.0):
+    """The served workload: Poisson arrivals (rate_hz jobs/s), scene uniform
+    over the 8 served scenes, resolution from {128,256,512,1024}^2, spp from
+    {4,16,64}, PT or BDPT 70/30.  Returns a list of dicts."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate_hz, n_jobs))
+    res = rng.choice([128, 256, 512, 1024], n_jobs)
+    spp = rng.choice([4, 16, 64], n_jobs)
+    scene = rng.integers(0, 8, n_jobs)
+    bdpt = rng.uniform(size=n_jobs) < 0.3
+    return [{"arrival_s": float(t[i]), "scene": int(scene[i]), "res": int(res[i]), "spp": int(spp[i]),
+             "integrator": "bdpt" if bdpt[i] else "pt"} for i in range(n_jobs)]
+
+
 def furnace(albedo=0.5, seed=0):
     """Closed Lambertian sphere of uniform albedo around a point light at its
     centre (an analytic check: every surface point sees irradiance I / r^2)."""

@@ -75,6 +75,11 @@ struct Workspace {
 
 namespace ar {
 
+struct PathEngine;
+void engine_destroy(PathEngine* e);
+struct BdptBatcher;
+void bdpt_destroy(BdptBatcher* b);
+
 // Optional per-kernel CUDA-event timing on the context stream.
 struct Profiler {
     bool on = false;
@@ -126,6 +131,9 @@ struct ar_context {
     uint64_t* stats_h = nullptr;  // pinned copy of stats_d, valid after a sync
     ar_render_stats last_stats{};
     bool stats_pending = false;
+    ar::PathEngine* engine = nullptr;  // streaming wavefront engine for ar_render
+    uint32_t engine_capacity = 1u << 21;
+    ar::BdptBatcher* bdpt = nullptr;   // BDPT batch buffers for ar_render
 };
 
 struct ar_scene {

@@ -1,9 +1,10 @@
 // Wavefront bidirectional path tracer (BidirectionalPathTracer::render,
-// src/integrators/bidirectional_path_tracer.rs:1221-1357).
+// src/integrators/bidirectional_path_tracer.rs:1221-1357), batched over jobs.
 //
-// Stages per chunk of camera samples:
+// A batch is a list of segments (job, first sample, count); the samples of all
+// segments are traced together.  Stages per batch:
 //   generate   camera vertex z0 + primary ray, light vertex y0 + emitted ray
-//   [extend -> vertex] x max_depth
+//   [extend -> vertex] x max depth of the batch
 //              both subpaths of every sample trace in one wavefront; each hit
 //              appends a vertex (area-measure pdf_fwd) and retroactively sets
 //              pdf_rev of the previous vertex (:338-559)
@@ -11,8 +12,8 @@
 //              s + t <= max_depth + 2, evaluates the unweighted contribution
 //              and the power-heuristic MIS weight (FP64 ratio walk, :594-770)
 //              and emits one shadow ray per candidate (:782-1155)
-//   shadow     any-hit test; visible contributions go to the film (s >= 2: the
-//              sample's pixel; s = 1: the projected splat pixel)
+//   shadow     any-hit test; visible contributions go to the job's film (s >= 2:
+//              the sample's pixel; s = 1: the projected splat pixel)
 // Vertices are stored SoA by (subpath, depth, sample) so each stage reads
 // coalesced 16-byte records.  Quad-light strategies (t = 0 and area-light t = 1)
 // are the same extension the oracle implements.
@@ -20,7 +21,10 @@
 
 #include <algorithm>
 #include <cmath>
+#include <memory>
+#include <vector>
 
+#include "ar_bdpt.hpp"
 #include "ar_shading.cuh"
 
 namespace cg = cooperative_groups;
@@ -32,36 +36,30 @@ namespace {
 constexpr uint32_t kTypeSurface = 0, kTypeCamera = 1, kTypeLight = 2;
 
 struct BdParams {
-    DevScene sc;
-    CameraDev cam;
-    uint32_t width, height, spp, max_depth, rr_depth, mis_mode;
-    float mis_beta;
-    uint32_t film64;
-    uint64_t seed;
-    uint64_t sample_begin;
-    uint32_t nsamples;  // samples in this chunk
-    uint32_t maxv;      // vertices per subpath (max_depth + 1)
-    float inv_spp;
-    void* film;
-    // vertices: index ((sub * maxv + k) * nsamples + si)
+    const BdJob* jobs;
+    const BdSegment* seg;
+    uint32_t nseg;
+    uint32_t nsamples;  // samples in this batch
+    uint32_t maxv;      // vertex capacity per subpath
+    uint32_t* sjob;     // job of each batch sample
+    unsigned long long* sindex;  // global sample index of each batch sample
     float4* va;  // p.xyz, pdf_fwd
     float4* vb;  // n.xyz, pdf_rev
     float4* vc;  // thr.xyz, info (type << 30 | delta << 29 | index)
     uint8_t* nv; // [sub * nsamples + si]
-    // tracing state per subpath q = 2 * si + sub
-    float4* thr;     // thr.xyz, previous directional pdf
+    float4* thr; // per subpath q = 2 si + sub: thr.xyz, previous directional pdf
     uint32_t* dim;
     float4* ray_o[2];
     float4* ray_d[2];
     uint32_t* qpath[2];
     float4* hit;
     uint32_t* hit_inst;
-    // connection shadow queue
     float4* sh_o;
     float4* sh_d;  // dir.xyz, tmax
     float4* sh_c;  // contribution.xyz, pixel bits
+    uint32_t* sh_job;
     uint32_t sh_cap;
-    uint32_t* counts;  // [0..max_depth]: rays per bounce; [64]: shadow rays; [65]: overflow flag
+    uint32_t* counts;  // [0..63]: rays per bounce; [64]: shadow rays; [65]: overflow flag
 };
 
 __device__ __forceinline__ size_t vidx(const BdParams& P, uint32_t sub, uint32_t k, uint32_t si) {
@@ -126,9 +124,9 @@ __device__ __forceinline__ f3 uniform_sphere(float ux, float uy) {
 __device__ __forceinline__ bool mis_delta(const Vtx& v) { return v.type == kTypeSurface && v.delta; }
 
 // mis_weight (:594-770) with the area-light extension for the t == 1 step.
-__device__ float mis_weight(const BdParams& P, uint32_t si, uint32_t S, uint32_t T, uint32_t s, uint32_t t,
-                            float pdf_cc, float pdf_cl) {
-    if (P.mis_mode == AR_MIS_UNIFORM) {
+__device__ float mis_weight(const BdParams& P, const BdJob& J, uint32_t si, uint32_t S, uint32_t T, uint32_t s,
+                            uint32_t t, float pdf_cc, float pdf_cl) {
+    if (J.mis_mode == AR_MIS_UNIFORM) {
         const uint32_t len = s + t;
         uint32_t count = 0;
         for (uint32_t t2 = 0; t2 <= min(len, T); ++t2) {
@@ -139,7 +137,7 @@ __device__ float mis_weight(const BdParams& P, uint32_t si, uint32_t S, uint32_t
         return count == 0 ? 1.0f : 1.0f / float(count);
     }
     if (s + t == 2) return 1.0f;
-    const double beta = double(P.mis_beta);
+    const double beta = double(J.mis_beta);
     auto pw = [&](double r) { return beta == 2.0 ? r * r : pow(r, beta); };
     double sum = 0.0;
     {
@@ -167,7 +165,7 @@ __device__ float mis_weight(const BdParams& P, uint32_t si, uint32_t S, uint32_t
                 pd = mis_delta(load_vtx(P, 1, t - 2, si));
             } else {
                 const Vtx y0 = load_vtx(P, 1, 0, si);
-                pd = P.sc.lights[y0.index].kind == AR_LIGHT_POINT;
+                pd = J.sc.lights[y0.index].kind == AR_LIGHT_POINT;
             }
             if (!mis_delta(v) && !pd) sum += pw(fabs(ri));
         }
@@ -181,21 +179,22 @@ __device__ float mis_weight(const BdParams& P, uint32_t si, uint32_t S, uint32_t
     return float(1.0 / (1.0 + sum));
 }
 
-__device__ __forceinline__ void film_add(const BdParams& P, uint32_t pix, f3 v) {
-    if (P.film64) {
-        double* f = static_cast<double*>(P.film) + 3 * size_t(pix);
+__device__ __forceinline__ void film_add(const BdJob& J, uint32_t pix, f3 v) {
+    if (J.film64) {
+        double* f = static_cast<double*>(J.film) + 3 * size_t(pix);
         atomicAdd(f, double(v.x));
         atomicAdd(f + 1, double(v.y));
         atomicAdd(f + 2, double(v.z));
     } else {
-        float* f = static_cast<float*>(P.film) + 3 * size_t(pix);
+        float* f = static_cast<float*>(J.film) + 3 * size_t(pix);
         atomicAdd(f, v.x);
         atomicAdd(f + 1, v.y);
         atomicAdd(f + 2, v.z);
     }
 }
 
-__device__ __forceinline__ void push_shadow(const BdParams& P, f3 o, f3 d, float tmax, f3 c, uint32_t pix) {
+__device__ __forceinline__ void push_shadow(const BdParams& P, uint32_t job, f3 o, f3 d, float tmax, f3 c,
+                                            uint32_t pix) {
     cg::coalesced_group g = cg::coalesced_threads();
     uint32_t base = 0;
     if (g.thread_rank() == 0) base = atomicAdd(&P.counts[64], g.size());
@@ -208,36 +207,46 @@ __device__ __forceinline__ void push_shadow(const BdParams& P, f3 o, f3 d, float
     P.sh_o[slot] = make_float4(o.x, o.y, o.z, 0.f);
     P.sh_d[slot] = make_float4(d.x, d.y, d.z, tmax);
     P.sh_c[slot] = make_float4(c.x, c.y, c.z, __uint_as_float(pix));
+    P.sh_job[slot] = job;
 }
 
 __global__ void __launch_bounds__(256) k_bd_generate(BdParams P) {
-    const uint32_t npix = P.width * P.height;
     for (uint32_t base = blockIdx.x * blockDim.x; base < 2 * P.nsamples; base += gridDim.x * blockDim.x) {
         const uint32_t q = base + threadIdx.x;
         bool live = q < 2 * P.nsamples;
         const uint32_t si = q >> 1, sub = q & 1u;
         Ray r{};
         if (live) {
-            const uint64_t g = P.sample_begin + si;
+            uint32_t lo = 0, hi = P.nseg;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (P.seg[mid].offset <= si) lo = mid; else hi = mid;
+            }
+            const BdSegment sg = P.seg[lo];
+            const BdJob& J = P.jobs[sg.job];
+            const unsigned long long g = sg.sample_begin + (si - sg.offset);
+            const uint32_t npix = J.width * J.height;
             const uint32_t pixel = uint32_t(g % npix), sample = uint32_t(g / npix);
-            const uint64_t key = counter_key(P.seed, pixel, sample);
+            const uint64_t key = counter_key(J.seed, pixel, sample);
             if (sub == 0) {
+                P.sjob[si] = sg.job;
+                P.sindex[si] = g;
                 const float jx = counter_u01(key, 0), jy = counter_u01(key, 1);
-                const uint32_t px = pixel % P.width, py = pixel / P.width;
-                r = camera_ray(P.cam, (float(px) + jx) / float(P.width), 1.0f - (float(py) + jy) / float(P.height));
-                store_vtx(P, 0, 0, si, ld3(P.cam.o), r.d, mk(1.f, 1.f, 1.f), 1.0f, kTypeCamera, true, 0);
+                const uint32_t px = pixel % J.width, py = pixel / J.width;
+                r = camera_ray(J.cam, (float(px) + jx) / float(J.width), 1.0f - (float(py) + jy) / float(J.height));
+                store_vtx(P, 0, 0, si, ld3(J.cam.o), r.d, mk(1.f, 1.f, 1.f), 1.0f, kTypeCamera, true, 0);
                 P.nv[si] = 1;
-                P.thr[q] = make_float4(1.f, 1.f, 1.f, camera_pdf_we(P.cam, r.d));
+                P.thr[q] = make_float4(1.f, 1.f, 1.f, camera_pdf_we(J.cam, r.d));
                 P.dim[q] = 2;
-            } else if (light_enabled(P.sc)) {
+            } else if (light_enabled(J.sc)) {
                 uint32_t d = kLightSubpathDim;
                 const float u_sel = counter_u01(key, d++);
                 const float upx = counter_u01(key, d++), upy = counter_u01(key, d++);
                 const float udx = counter_u01(key, d++), udy = counter_u01(key, d++);
                 uint32_t li;
                 float sel;
-                light_select(P.sc, u_sel, li, sel);
-                const LightView L = load_light(P.sc, li);
+                light_select(J.sc, u_sel, li, sel);
+                const LightView L = load_light(J.sc, li);
                 f3 o, dir, nl;
                 float pdf_pos, pdf_dir;
                 bool ok = true;
@@ -250,8 +259,7 @@ __global__ void __launch_bounds__(256) k_bd_generate(BdParams P) {
                 } else {
                     o = (L.pos + L.e1 * upx) + L.e2 * upy;
                     const f3 local = cosine_hemisphere(udx, udy);
-                    const Onb f = onb_from_normal(L.n);
-                    dir = to_world(f, local);
+                    dir = to_world(onb_from_normal(L.n), local);
                     pdf_pos = 1.0f / L.area;
                     pdf_dir = local.z * kInvPi;
                     nl = L.n;
@@ -274,7 +282,7 @@ __global__ void __launch_bounds__(256) k_bd_generate(BdParams P) {
                 P.nv[P.nsamples + si] = 0;
                 live = false;
             }
-            if (P.max_depth == 0) live = false;
+            if (J.max_depth == 0) live = false;
         }
         const uint32_t slot = warp_alloc(&P.counts[0], live);
         if (!live) continue;
@@ -289,8 +297,9 @@ __global__ void __launch_bounds__(128) k_bd_extend(BdParams P, uint32_t depth, i
     const int b = depth & 1;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
         const float4 a = P.ray_o[b][j], d = P.ray_d[b][j];
+        const BdJob& J = P.jobs[P.sjob[P.qpath[b][j] >> 1]];
         HitRec h;
-        traverse<false>(P.sc, Ray{mk(a.x, a.y, a.z), mk(d.x, d.y, d.z), a.w, d.w}, h, err);
+        traverse<false>(J.sc, Ray{mk(a.x, a.y, a.z), mk(d.x, d.y, d.z), a.w, d.w}, h, err);
         P.hit[j] = make_float4(h.t, h.u, h.v, __uint_as_float(h.slot));
         P.hit_inst[j] = h.inst;
     }
@@ -308,13 +317,14 @@ __global__ void __launch_bounds__(256) k_bd_vertex(BdParams P, uint32_t depth) {
         if (j < n) {
             q = P.qpath[b][j];
             const uint32_t si = q >> 1, sub = q & 1u;
+            const BdJob& J = P.jobs[P.sjob[si]];
             const float4 h = P.hit[j];
             const uint32_t slot = __float_as_uint(h.w);
             if (slot != kInvalid) {
                 const float4 ro4 = P.ray_o[b][j], rd4 = P.ray_d[b][j];
                 const f3 ro = mk(ro4.x, ro4.y, ro4.z), rd = mk(rd4.x, rd4.y, rd4.z);
-                const Shade s = make_shade(P.sc, ro, rd, h.x, h.y, h.z, slot, P.hit_inst[j]);
-                const MatView m = load_mat(P.sc, s.mat);
+                const Shade s = make_shade(J.sc, ro, rd, h.x, h.y, h.z, slot, P.hit_inst[j]);
+                const MatView m = load_mat(J.sc, s.mat);
                 const float4 t4 = P.thr[q];
                 f3 thr = mk(t4.x, t4.y, t4.z);
                 const uint32_t k = P.nv[sub * P.nsamples + si];  // index of the new vertex
@@ -324,9 +334,9 @@ __global__ void __launch_bounds__(256) k_bd_vertex(BdParams P, uint32_t depth) {
                 const float pdf_fwd = pdf_sa_to_area(t4.w, prev_p, s.p, s.n);
                 store_vtx(P, sub, k, si, s.p, s.n, thr, pdf_fwd, kTypeSurface, false, s.mat);
                 P.nv[sub * P.nsamples + si] = uint8_t(k + 1);
-                const uint64_t g = P.sample_begin + si;
-                const uint32_t npix = P.width * P.height;
-                const uint64_t key = counter_key(P.seed, uint32_t(g % npix), uint32_t(g / npix));
+                const unsigned long long g = P.sindex[si];
+                const uint32_t npix = J.width * J.height;
+                const uint64_t key = counter_key(J.seed, uint32_t(g % npix), uint32_t(g / npix));
                 uint32_t d = P.dim[q];
                 const f3 wo_l = to_local(s.onb, -rd);
                 d++;  // u_sel (unused by these BSDFs)
@@ -338,12 +348,12 @@ __global__ void __launch_bounds__(256) k_bd_vertex(BdParams P, uint32_t depth) {
                     const float pdf_rev_dir = bsdf_pdf(m, wo_l, wi);
                     P.vb[pi].w = pdf_sa_to_area(pdf_rev_dir, s.p, prev_p, prev_n);
                     bool alive = true;
-                    if (depth + 1 >= P.rr_depth) {
+                    if (depth + 1 >= J.rr_depth) {
                         const float survival = fminf(max3(thr), 0.95f);
                         if (counter_u01(key, d++) > survival || survival <= 0.f) alive = false;
                         else thr = thr / survival;
                     }
-                    if (alive && depth + 1 < P.max_depth) {
+                    if (alive && depth + 1 < J.max_depth) {
                         const f3 wi_w = to_world(s.onb, wi);
                         no = s.p + (s.n * 1e-4f) * signum(dot(wi_w, s.n));
                         nd = normalize(wi_w);
@@ -365,21 +375,21 @@ __global__ void __launch_bounds__(256) k_bd_vertex(BdParams P, uint32_t depth) {
 
 // connect_bdpt for s >= 2 (:782-1044) + the t == 0 extension.  Emits a shadow
 // ray with the MIS-weighted contribution, or deposits directly when t == 0.
-__device__ void connect_general(const BdParams& P, uint32_t si, uint32_t S, uint32_t T, uint32_t s, uint32_t t,
-                                uint32_t pix) {
+__device__ void connect_general(const BdParams& P, const BdJob& J, uint32_t job, uint32_t si, uint32_t S, uint32_t T,
+                                uint32_t s, uint32_t t, uint32_t pix) {
     const Vtx z = load_vtx(P, 0, s - 1, si);
     const Vtx zp = load_vtx(P, 0, s - 2, si);
     if (t == 0) {
-        const MatView mz = load_mat(P.sc, z.index);
-        if (mz.emitter < 0 || !light_enabled(P.sc)) return;
-        const LightView lt = load_light(P.sc, uint32_t(mz.emitter));
+        const MatView mz = load_mat(J.sc, z.index);
+        if (mz.emitter < 0 || !light_enabled(J.sc)) return;
+        const LightView lt = load_light(J.sc, uint32_t(mz.emitter));
         const f3 wo = normalize(zp.p - z.p);
         if (dot(lt.n, wo) <= 0.f) return;
         const f3 c = z.thr * lt.inten;
         if (max3(c) <= 0.f) return;
-        const float pdf_cc = light_pmf_of(P.sc, uint32_t(mz.emitter)) / lt.area;
-        const float w = mis_weight(P, si, S, T, s, 0, pdf_cc, 0.f);
-        film_add(P, pix, (c * w) * P.inv_spp);
+        const float pdf_cc = light_pmf_of(J.sc, uint32_t(mz.emitter)) / lt.area;
+        const float w = mis_weight(P, J, si, S, T, s, 0, pdf_cc, 0.f);
+        film_add(J, pix, (c * w) * J.inv_spp);
         return;
     }
     const Vtx y = load_vtx(P, 1, t - 1, si);
@@ -396,7 +406,7 @@ __device__ void connect_general(const BdParams& P, uint32_t si, uint32_t S, uint
     const float sdist = length(sd);
     if (sdist < 1e-6f) return;
     const Onb oz = onb_from_normal(z.n);
-    const MatView mz = load_mat(P.sc, z.index);
+    const MatView mz = load_mat(J.sc, z.index);
     const f3 wo_z = normalize(zp.p - z.p);
     const f3 wo_zl = to_local(oz, wo_z);
     const f3 f_z = bsdf_eval(mz, to_local(oz, wi_z), wo_zl);
@@ -407,7 +417,7 @@ __device__ void connect_general(const BdParams& P, uint32_t si, uint32_t S, uint
     f3 wo_yl = mk(0.f, 0.f, 0.f);
     if (t != 1) {
         oy = onb_from_normal(y.n);
-        my = load_mat(P.sc, y.index);
+        my = load_mat(J.sc, y.index);
         const Vtx yp = load_vtx(P, 1, t - 2, si);
         wo_yl = to_local(oy, normalize(yp.p - y.p));
         f_y = bsdf_eval(my, to_local(oy, wi_y), wo_yl);
@@ -416,7 +426,7 @@ __device__ void connect_general(const BdParams& P, uint32_t si, uint32_t S, uint
     const float g = geometry_term(z.p, z.n, y.p, y.n);
     f3 c;
     if (t == 1) {
-        const LightView L = load_light(P.sc, y.index);
+        const LightView L = load_light(J.sc, y.index);
         if (L.kind == AR_LIGHT_POINT) {
             // :951-967 — re-sample the point light toward z
             f3 lwi, lrad;
@@ -434,42 +444,43 @@ __device__ void connect_general(const BdParams& P, uint32_t si, uint32_t S, uint
     if (max3(c) <= 0.f) return;
     float pdf_cc;
     if (t == 1) {
-        const LightView L = load_light(P.sc, y.index);
+        const LightView L = load_light(J.sc, y.index);
         pdf_cc = pdf_sa_to_area(light_pdf_emission_dir(L, normalize(z.p - y.p)), y.p, z.p, z.n);
     } else {
         const f3 wiy = normalize(z.p - y.p);
         pdf_cc = pdf_sa_to_area(bsdf_pdf(my, to_local(oy, wiy), wo_yl), y.p, z.p, z.n);
     }
     const float pdf_cl = pdf_sa_to_area(bsdf_pdf(mz, to_local(oz, normalize(y.p - z.p)), wo_zl), z.p, y.p, y.n);
-    const float w = mis_weight(P, si, S, T, s, t, pdf_cc, pdf_cl);
-    push_shadow(P, so, normalize(sd / sdist), sdist * (1.0f - 1e-4f), c * w, pix);
+    const float w = mis_weight(P, J, si, S, T, s, t, pdf_cc, pdf_cl);
+    push_shadow(P, job, so, normalize(sd / sdist), sdist * (1.0f - 1e-4f), c * w, pix);
 }
 
 // connect_bdpt_s1 (:1051-1155): light tracing to the pinhole, splatted.
-__device__ void connect_s1(const BdParams& P, uint32_t si, uint32_t S, uint32_t T, uint32_t t) {
+__device__ void connect_s1(const BdParams& P, const BdJob& J, uint32_t job, uint32_t si, uint32_t S, uint32_t T,
+                           uint32_t t) {
     const Vtx y = load_vtx(P, 1, t - 1, si);
     if (y.type == kTypeSurface && y.delta) return;
     // PinholeCamera::sample_we (src/cameras.rs:175-240)
-    const f3 co = ld3(P.cam.o);
+    const f3 co = ld3(J.cam.o);
     const f3 to_cam0 = co - y.p;
     const float d2 = dot(to_cam0, to_cam0);
     const float dist = sqrtf(d2);
     if (dist < 1e-6f) return;
     const f3 wi = to_cam0 / dist;
     const f3 dir = -wi;
-    const float ct = dot(dir, ld3(P.cam.fwd));
+    const float ct = dot(dir, ld3(J.cam.fwd));
     if (ct <= 1e-6f) return;
     const f3 ds = dir / ct;
-    const float u = dot(ds, ld3(P.cam.right)) / P.cam.vw + 0.5f;
-    const float v = dot(ds, ld3(P.cam.up)) / P.cam.vh + 0.5f;
+    const float u = dot(ds, ld3(J.cam.right)) / J.cam.vw + 0.5f;
+    const float v = dot(ds, ld3(J.cam.up)) / J.cam.vh + 0.5f;
     if (u < 0.f || u > 1.f || v < 0.f || v > 1.f) return;
-    const float px = u * float(P.width);
-    const float py = (1.0f - v) * float(P.height);
-    if (px < 0.f || px >= float(P.width) || py < 0.f || py >= float(P.height)) return;
+    const float px = u * float(J.width);
+    const float py = (1.0f - v) * float(J.height);
+    if (px < 0.f || px >= float(J.width) || py < 0.f || py >= float(J.height)) return;
     const float c2 = ct * ct, c4 = c2 * c2;
-    const float we = 1.0f / (P.cam.area * c4);
+    const float we = 1.0f / (J.cam.area * c4);
     const Onb oy = onb_from_normal(y.n);
-    const MatView my = load_mat(P.sc, y.index);
+    const MatView my = load_mat(J.sc, y.index);
     const Vtx yp = load_vtx(P, 1, t - 2, si);
     const f3 wo_yl = to_local(oy, normalize(yp.p - y.p));
     const f3 f_y = bsdf_eval(my, to_local(oy, wi), wo_yl);
@@ -479,26 +490,27 @@ __device__ void connect_s1(const BdParams& P, uint32_t si, uint32_t S, uint32_t 
     if (max3(c) <= 0.f) return;
     const Vtx z0 = load_vtx(P, 0, 0, si);
     const float pdf_cl = pdf_sa_to_area(bsdf_pdf(my, to_local(oy, wi), wo_yl), y.p, co, z0.n);
-    const float w = mis_weight(P, si, S, T, 1, t, 0.f, pdf_cl);
-    const uint32_t ix = min(uint32_t(px), P.width - 1), iy = min(uint32_t(py), P.height - 1);
+    const float w = mis_weight(P, J, si, S, T, 1, t, 0.f, pdf_cl);
+    const uint32_t ix = min(uint32_t(px), J.width - 1), iy = min(uint32_t(py), J.height - 1);
     const f3 o = y.p + (y.n * 1e-4f) * signum(dot(wi, y.n));
-    push_shadow(P, o, normalize(wi), dist * (1.0f - 1e-4f), c * w, iy * P.width + ix);
+    push_shadow(P, job, o, normalize(wi), dist * (1.0f - 1e-4f), c * w, iy * J.width + ix);
 }
 
 __global__ void __launch_bounds__(128) k_bd_connect(BdParams P) {
-    const uint32_t npix = P.width * P.height;
     for (uint32_t si = blockIdx.x * blockDim.x + threadIdx.x; si < P.nsamples; si += gridDim.x * blockDim.x) {
+        const uint32_t job = P.sjob[si];
+        const BdJob& J = P.jobs[job];
         const uint32_t S = P.nv[si], T = P.nv[P.nsamples + si];
-        const uint32_t pix = uint32_t((P.sample_begin + si) % npix);
-        const uint32_t limit = P.max_depth + 2;
+        const uint32_t pix = uint32_t(P.sindex[si] % (J.width * J.height));
+        const uint32_t limit = J.max_depth + 2;
         for (uint32_t t = 0; t <= T; ++t)
             for (uint32_t s = 1; s <= S; ++s) {
                 if (s + t < 2 || s + t > limit) continue;
                 if (s == 1) {
-                    if (t >= 2) connect_s1(P, si, S, T, t);
+                    if (t >= 2) connect_s1(P, J, job, si, S, T, t);
                     continue;
                 }
-                connect_general(P, si, S, T, s, t, pix);
+                connect_general(P, J, job, si, S, T, s, t, pix);
             }
     }
 }
@@ -507,11 +519,12 @@ __global__ void __launch_bounds__(128) k_bd_shadow(BdParams P, int* err) {
     const uint32_t n = min(P.counts[64], P.sh_cap);
     for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
         const float4 a = P.sh_o[m], d = P.sh_d[m];
+        const BdJob& J = P.jobs[P.sh_job[m]];
         HitRec h;
-        traverse<true>(P.sc, Ray{mk(a.x, a.y, a.z), mk(d.x, d.y, d.z), 0.f, d.w}, h, err);
+        traverse<true>(J.sc, Ray{mk(a.x, a.y, a.z), mk(d.x, d.y, d.z), 0.f, d.w}, h, err);
         if (h.slot == kInvalid) {
             const float4 c = P.sh_c[m];
-            film_add(P, __float_as_uint(c.w), mk(c.x, c.y, c.z) * P.inv_spp);
+            film_add(J, __float_as_uint(c.w), mk(c.x, c.y, c.z) * J.inv_spp);
         }
     }
 }
@@ -535,101 +548,191 @@ T* carve(char*& cur, size_t n) {
     return p;
 }
 
+uint32_t max_pairs_for(uint32_t max_depth) {
+    const uint32_t maxv = max_depth + 1;
+    uint32_t n = 0;
+    for (uint32_t t = 0; t <= maxv; ++t)
+        for (uint32_t s = 1; s <= maxv; ++s)
+            if (s + t >= 2 && s + t <= max_depth + 2) n++;
+    return n;
+}
+
 }  // namespace
 
+struct BdptBatcher {
+    ar_context* ctx;
+    uint32_t max_depth_cap, batch;
+    DevBuf mem, jobs_d, seg_d;
+    BdParams P{};
+    BdJob* jobs_h = nullptr;      // pinned staging
+    BdSegment* seg_h = nullptr;   // pinned staging
+    cudaEvent_t staged = nullptr;
+};
+
+size_t bdpt_batch_bytes(uint32_t max_depth, uint32_t batch) {
+    const size_t maxv = max_depth + 1;
+    const size_t per_sample = 2 * maxv * 48 + 2 + 2 * (16 + 4) + 2 * 2 * (32 + 4) + 2 * 20 + 4 + 8 +
+                              size_t(max_pairs_for(max_depth)) * 52;
+    return per_sample * batch + 64 * 1024;
+}
+
+BdptBatcher* bdpt_create(ar_context* ctx, uint32_t max_depth_cap, uint32_t batch) {
+    AR_REQUIRE(max_depth_cap <= 62, AR_ERR_INVALID_ARGUMENT, "BDPT max_depth must be <= 62");
+    auto b = std::make_unique<BdptBatcher>();
+    b->ctx = ctx;
+    b->max_depth_cap = max_depth_cap;
+    b->batch = batch;
+    b->mem.alloc(bdpt_batch_bytes(max_depth_cap, batch));
+    b->jobs_d.alloc(kMaxBdptJobs * sizeof(BdJob));
+    b->seg_d.alloc(kMaxBdptJobs * sizeof(BdSegment));
+    AR_CUDA(cudaMallocHost(&b->jobs_h, kMaxBdptJobs * sizeof(BdJob)));
+    AR_CUDA(cudaMallocHost(&b->seg_h, kMaxBdptJobs * sizeof(BdSegment)));
+    AR_CUDA(cudaEventCreateWithFlags(&b->staged, cudaEventDisableTiming));
+    AR_CUDA(cudaEventRecord(b->staged, ctx->stream));
+    char* cur = b->mem.as<char>();
+    BdParams& P = b->P;
+    const uint32_t maxv = max_depth_cap + 1;
+    P.maxv = maxv;
+    const size_t nvtx = size_t(2) * maxv * batch;
+    P.va = carve<float4>(cur, nvtx);
+    P.vb = carve<float4>(cur, nvtx);
+    P.vc = carve<float4>(cur, nvtx);
+    P.nv = carve<uint8_t>(cur, 2 * size_t(batch));
+    P.thr = carve<float4>(cur, 2 * size_t(batch));
+    P.dim = carve<uint32_t>(cur, 2 * size_t(batch));
+    for (int k = 0; k < 2; ++k) {
+        P.ray_o[k] = carve<float4>(cur, 2 * size_t(batch));
+        P.ray_d[k] = carve<float4>(cur, 2 * size_t(batch));
+        P.qpath[k] = carve<uint32_t>(cur, 2 * size_t(batch));
+    }
+    P.hit = carve<float4>(cur, 2 * size_t(batch));
+    P.hit_inst = carve<uint32_t>(cur, 2 * size_t(batch));
+    P.sjob = carve<uint32_t>(cur, batch);
+    P.sindex = carve<unsigned long long>(cur, batch);
+    P.sh_cap = uint32_t(std::min<uint64_t>(uint64_t(max_pairs_for(max_depth_cap)) * batch, 0xFFFFFFF0ull));
+    P.sh_o = carve<float4>(cur, P.sh_cap);
+    P.sh_d = carve<float4>(cur, P.sh_cap);
+    P.sh_c = carve<float4>(cur, P.sh_cap);
+    P.sh_job = carve<uint32_t>(cur, P.sh_cap);
+    P.counts = carve<uint32_t>(cur, 128);
+    P.jobs = b->jobs_d.as<BdJob>();
+    P.seg = b->seg_d.as<BdSegment>();
+    return b.release();
+}
+
+void bdpt_destroy(BdptBatcher* b) {
+    if (!b) return;
+    if (b->jobs_h) cudaFreeHost(b->jobs_h);
+    if (b->seg_h) cudaFreeHost(b->seg_h);
+    if (b->staged) cudaEventDestroy(b->staged);
+    delete b;
+}
+
+uint32_t bdpt_batch_capacity(const BdptBatcher* b) { return b->batch; }
+uint32_t bdpt_max_depth_cap(const BdptBatcher* b) { return b->max_depth_cap; }
+
+void bdpt_run_batch(BdptBatcher* b, const std::vector<BdJob>& jobs, const std::vector<BdSegment>& segs) {
+    ar_context* ctx = b->ctx;
+    AR_REQUIRE(!segs.empty() && segs.size() <= kMaxBdptJobs && jobs.size() <= kMaxBdptJobs, AR_ERR_INVALID_ARGUMENT,
+               "bad BDPT batch");
+    uint32_t nsamples = 0, max_depth = 0;
+    for (const auto& s : segs) nsamples = std::max(nsamples, s.offset + s.nsamples);
+    for (const auto& j : jobs) {
+        AR_REQUIRE(j.max_depth <= b->max_depth_cap, AR_ERR_INVALID_ARGUMENT, "job max_depth above the batch capacity");
+        max_depth = std::max(max_depth, j.max_depth);
+    }
+    AR_REQUIRE(nsamples <= b->batch, AR_ERR_INVALID_ARGUMENT, "batch too large");
+    AR_CUDA(cudaEventSynchronize(b->staged));  // staging buffers free again
+    std::copy(jobs.begin(), jobs.end(), b->jobs_h);
+    std::copy(segs.begin(), segs.end(), b->seg_h);
+    AR_CUDA(cudaMemcpyAsync(b->jobs_d.ptr, b->jobs_h, jobs.size() * sizeof(BdJob), cudaMemcpyHostToDevice,
+                            ctx->stream));
+    AR_CUDA(cudaMemcpyAsync(b->seg_d.ptr, b->seg_h, segs.size() * sizeof(BdSegment), cudaMemcpyHostToDevice,
+                            ctx->stream));
+    AR_CUDA(cudaEventRecord(b->staged, ctx->stream));
+    BdParams P = b->P;
+    P.nseg = uint32_t(segs.size());
+    P.nsamples = nsamples;
+    int* err = ctx->err_flag.as<int>();
+    const int wide = ctx->num_sms * 8;
+    AR_CUDA(cudaMemsetAsync(P.counts, 0, 128 * sizeof(uint32_t), ctx->stream));
+    {
+        KernelScope ks(ctx->prof, ctx->stream, "bdpt_generate");
+        k_bd_generate<<<std::max(1, int(std::min<uint64_t>((2ull * nsamples + 255) / 256, wide))), 256, 0,
+                        ctx->stream>>>(P);
+    }
+    for (uint32_t d = 0; d < max_depth; ++d) {
+        {
+            KernelScope ks(ctx->prof, ctx->stream, "bdpt_extend");
+            k_bd_extend<<<ctx->num_sms * 16, 128, 0, ctx->stream>>>(P, d, err);
+        }
+        {
+            KernelScope ks(ctx->prof, ctx->stream, "bdpt_vertex");
+            k_bd_vertex<<<wide, 256, 0, ctx->stream>>>(P, d);
+        }
+    }
+    {
+        KernelScope ks(ctx->prof, ctx->stream, "bdpt_connect");
+        k_bd_connect<<<std::max(1, int(std::min<uint64_t>((nsamples + 127) / 128, ctx->num_sms * 16))), 128, 0,
+                       ctx->stream>>>(P);
+    }
+    {
+        KernelScope ks(ctx->prof, ctx->stream, "bdpt_shadow");
+        k_bd_shadow<<<ctx->num_sms * 16, 128, 0, ctx->stream>>>(P, err);
+    }
+    k_bd_count<<<1, 32, 0, ctx->stream>>>(P.counts, max_depth, ctx->stats_d.as<unsigned long long>(), err);
+    AR_CUDA(cudaGetLastError());
+}
+
+BdJob make_bdpt_job(const ar_scene* sc, const CameraDev& cam, const ar_integrator_cfg& cfg, uint32_t w, uint32_t h,
+                    void* film) {
+    BdJob J{};
+    J.sc = sc->view;
+    J.cam = cam;
+    J.width = w;
+    J.height = h;
+    J.spp = cfg.spp;
+    J.max_depth = cfg.max_depth;
+    J.rr_depth = cfg.rr_depth;
+    J.mis_mode = cfg.mis_mode;
+    J.mis_beta = cfg.mis_beta;
+    J.film64 = cfg.film_precision == AR_FILM_F64 ? 1u : 0u;
+    J.seed = cfg.seed;
+    J.inv_spp = 1.0f / float(cfg.spp);
+    J.film = film;
+    return J;
+}
+
+// Single-job BDPT render (the plain path): consecutive batches of one job.
 void render_bdpt_film(ar_context* ctx, const ar_scene* sc, const CameraDev& cam, const ar_integrator_cfg& cfg,
                       uint32_t w, uint32_t h, void* film) {
     AR_REQUIRE(cfg.max_depth <= 62, AR_ERR_INVALID_ARGUMENT, "max_depth must be <= 62");
     const uint64_t total = uint64_t(w) * h * cfg.spp;
-    const uint32_t maxv = cfg.max_depth + 1;
-    // Worst-case connections per sample: (s, t) pairs with 1 <= s, t <= maxv, s + t <= max_depth + 2.
-    uint32_t max_pairs = 0;
-    for (uint32_t t = 0; t <= maxv; ++t)
-        for (uint32_t s = 1; s <= maxv; ++s)
-            if (s + t >= 2 && s + t <= cfg.max_depth + 2) max_pairs++;
-    const size_t per_sample = size_t(2) * maxv * 48 + 2 + 2 * (16 + 4) + 2 * 2 * (32 + 4) + 2 * 20 +
-                              size_t(max_pairs) * 48;
     const size_t budget = size_t(3) << 30;
-    const uint32_t chunk = uint32_t(std::max<uint64_t>(1024, std::min<uint64_t>(total, budget / per_sample)));
-    ctx->work.ensure(per_sample * chunk + 64 * 1024);
-    char* cur = ctx->work.buf.as<char>();
-    BdParams P{};
-    P.sc = sc->view;
-    P.cam = cam;
-    P.width = w;
-    P.height = h;
-    P.spp = cfg.spp;
-    P.max_depth = cfg.max_depth;
-    P.rr_depth = cfg.rr_depth;
-    P.mis_mode = cfg.mis_mode;
-    P.mis_beta = cfg.mis_beta;
-    P.film64 = cfg.film_precision == AR_FILM_F64 ? 1u : 0u;
-    P.seed = cfg.seed;
-    P.maxv = maxv;
-    P.inv_spp = 1.0f / float(cfg.spp);
-    P.film = film;
-    const size_t nvtx = size_t(2) * maxv * chunk;
-    P.va = carve<float4>(cur, nvtx);
-    P.vb = carve<float4>(cur, nvtx);
-    P.vc = carve<float4>(cur, nvtx);
-    P.nv = carve<uint8_t>(cur, 2 * size_t(chunk));
-    P.thr = carve<float4>(cur, 2 * size_t(chunk));
-    P.dim = carve<uint32_t>(cur, 2 * size_t(chunk));
-    for (int b = 0; b < 2; ++b) {
-        P.ray_o[b] = carve<float4>(cur, 2 * size_t(chunk));
-        P.ray_d[b] = carve<float4>(cur, 2 * size_t(chunk));
-        P.qpath[b] = carve<uint32_t>(cur, 2 * size_t(chunk));
+    const size_t per = bdpt_batch_bytes(cfg.max_depth, 1024) / 1024 + 1;
+    const uint32_t batch = uint32_t(std::max<uint64_t>(1024, std::min<uint64_t>(total, budget / per)));
+    if (!ctx->bdpt || bdpt_max_depth_cap(ctx->bdpt) < cfg.max_depth || bdpt_batch_capacity(ctx->bdpt) < batch) {
+        AR_CUDA(cudaStreamSynchronize(ctx->stream));
+        bdpt_destroy(ctx->bdpt);
+        ctx->bdpt = nullptr;
+        ctx->bdpt = bdpt_create(ctx, std::max(cfg.max_depth, 10u), batch);
     }
-    P.hit = carve<float4>(cur, 2 * size_t(chunk));
-    P.hit_inst = carve<uint32_t>(cur, 2 * size_t(chunk));
-    P.sh_cap = uint32_t(std::min<uint64_t>(uint64_t(max_pairs) * chunk, 0xFFFFFFF0ull));
-    P.sh_o = carve<float4>(cur, P.sh_cap);
-    P.sh_d = carve<float4>(cur, P.sh_cap);
-    P.sh_c = carve<float4>(cur, P.sh_cap);
-    P.counts = carve<uint32_t>(cur, 128);
-    const size_t film_bytes = size_t(w) * h * 3 * (P.film64 ? sizeof(double) : sizeof(float));
-    AR_CUDA(cudaMemsetAsync(film, 0, film_bytes, ctx->stream));
+    const bool f64 = cfg.film_precision == AR_FILM_F64;
+    AR_CUDA(cudaMemsetAsync(film, 0, size_t(w) * h * 3 * (f64 ? sizeof(double) : sizeof(float)), ctx->stream));
     AR_CUDA(cudaMemsetAsync(ctx->stats_d.ptr, 0, 8 * sizeof(uint64_t), ctx->stream));
-    int* err = ctx->err_flag.as<int>();
-    const int wide = ctx->num_sms * 8;
-    uint64_t chunks = 0;
-    for (uint64_t begin = 0; begin < total; begin += chunk, ++chunks) {
-        P.sample_begin = begin;
-        P.nsamples = uint32_t(std::min<uint64_t>(chunk, total - begin));
-        AR_CUDA(cudaMemsetAsync(P.counts, 0, 128 * sizeof(uint32_t), ctx->stream));
-        {
-            KernelScope ks(ctx->prof, ctx->stream, "bdpt_generate");
-            k_bd_generate<<<std::max(1, int(std::min<uint64_t>((2ull * P.nsamples + 255) / 256, wide))), 256, 0,
-                            ctx->stream>>>(P);
-        }
-        for (uint32_t d = 0; d < cfg.max_depth; ++d) {
-            {
-                KernelScope ks(ctx->prof, ctx->stream, "bdpt_extend");
-                k_bd_extend<<<ctx->num_sms * 16, 128, 0, ctx->stream>>>(P, d, err);
-            }
-            {
-                KernelScope ks(ctx->prof, ctx->stream, "bdpt_vertex");
-                k_bd_vertex<<<wide, 256, 0, ctx->stream>>>(P, d);
-            }
-        }
-        {
-            KernelScope ks(ctx->prof, ctx->stream, "bdpt_connect");
-            k_bd_connect<<<std::max(1, int(std::min<uint64_t>((P.nsamples + 127) / 128, ctx->num_sms * 16))), 128, 0,
-                           ctx->stream>>>(P);
-        }
-        {
-            KernelScope ks(ctx->prof, ctx->stream, "bdpt_shadow");
-            k_bd_shadow<<<ctx->num_sms * 16, 128, 0, ctx->stream>>>(P, err);
-        }
-        k_bd_count<<<1, 32, 0, ctx->stream>>>(P.counts, cfg.max_depth, ctx->stats_d.as<unsigned long long>(), err);
-        AR_CUDA(cudaGetLastError());
+    const std::vector<BdJob> jobs{make_bdpt_job(sc, cam, cfg, w, h, film)};
+    const uint32_t cap = bdpt_batch_capacity(ctx->bdpt);
+    uint64_t batches = 0;
+    for (uint64_t begin = 0; begin < total; begin += cap, ++batches) {
+        const uint32_t n = uint32_t(std::min<uint64_t>(cap, total - begin));
+        bdpt_run_batch(ctx->bdpt, jobs, {BdSegment{0, 0, n, 0, begin}});
     }
     AR_CUDA(cudaMemcpyAsync(ctx->stats_h, ctx->stats_d.ptr, 8 * sizeof(uint64_t), cudaMemcpyDeviceToHost,
                             ctx->stream));
     ctx->stats_pending = true;
     ctx->last_stats.path_samples = total;
-    ctx->last_stats.extend_launches = chunks * cfg.max_depth;
-    ctx->last_stats.shadow_launches = chunks;
+    ctx->last_stats.extend_launches = batches * cfg.max_depth;
+    ctx->last_stats.shadow_launches = batches;
 }
 
 }  // namespace ar

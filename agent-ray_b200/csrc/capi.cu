@@ -32,6 +32,38 @@ void check_device_flag(ar_context* ctx) {
     }
 }
 
+ar_context* context_create_internal(int device) {
+    int count = 0;
+    AR_CUDA(cudaGetDeviceCount(&count));
+    AR_REQUIRE(device >= 0 && device < count, AR_ERR_INVALID_ARGUMENT, "no such CUDA device");
+    AR_CUDA(cudaSetDevice(device));
+    auto ctx = std::make_unique<ar_context>();
+    ctx->device = device;
+    AR_CUDA(cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking));
+    ctx->stream = ctx->own_stream;
+    AR_CUDA(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device));
+    ctx->err_flag.alloc(64);
+    AR_CUDA(cudaMemset(ctx->err_flag.ptr, 0, 64));
+    ctx->stats_d.alloc(8 * sizeof(uint64_t));
+    AR_CUDA(cudaMemset(ctx->stats_d.ptr, 0, 8 * sizeof(uint64_t)));
+    AR_CUDA(cudaMallocHost(&ctx->stats_h, 8 * sizeof(uint64_t)));
+    std::memset(ctx->stats_h, 0, 8 * sizeof(uint64_t));
+    return ctx.release();
+}
+
+void context_destroy_internal(ar_context* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->engine) engine_destroy(ctx->engine);
+    ctx->engine = nullptr;
+    bdpt_destroy(ctx->bdpt);
+    ctx->bdpt = nullptr;
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    if (ctx->stats_h) cudaFreeHost(ctx->stats_h);
+    delete ctx;
+}
+
 }  // namespace ar
 
 using namespace ar;
@@ -45,34 +77,12 @@ int ar_abi_version(void) { return AR_ABI_VERSION; }
 int ar_context_create(int device, ar_context** out) {
     return guarded([&] {
         AR_REQUIRE(out, AR_ERR_INVALID_ARGUMENT, "out is null");
-        int count = 0;
-        AR_CUDA(cudaGetDeviceCount(&count));
-        AR_REQUIRE(device >= 0 && device < count, AR_ERR_INVALID_ARGUMENT, "no such CUDA device");
-        AR_CUDA(cudaSetDevice(device));
-        auto ctx = std::make_unique<ar_context>();
-        ctx->device = device;
-        AR_CUDA(cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking));
-        ctx->stream = ctx->own_stream;
-        AR_CUDA(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device));
-        ctx->err_flag.alloc(64);
-        AR_CUDA(cudaMemset(ctx->err_flag.ptr, 0, 64));
-        ctx->stats_d.alloc(8 * sizeof(uint64_t));
-        AR_CUDA(cudaMemset(ctx->stats_d.ptr, 0, 8 * sizeof(uint64_t)));
-        AR_CUDA(cudaMallocHost(&ctx->stats_h, 8 * sizeof(uint64_t)));
-        std::memset(ctx->stats_h, 0, 8 * sizeof(uint64_t));
-        *out = ctx.release();
+        *out = context_create_internal(device);
     });
 }
 
 int ar_context_destroy(ar_context* ctx) {
-    return guarded([&] {
-        if (!ctx) return;
-        cudaSetDevice(ctx->device);
-        if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-        if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
-        if (ctx->stats_h) cudaFreeHost(ctx->stats_h);
-        delete ctx;
-    });
+    return guarded([&] { context_destroy_internal(ctx); });
 }
 
 int ar_context_set_stream(ar_context* ctx, void* stream) {

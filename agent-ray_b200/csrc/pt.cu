@@ -1,200 +1,243 @@
-// Wavefront path tracer: PathTracer::li / render (src/integrators/path_tracer.rs:59-190)
-// and the base/offset paths of the gradient-domain tracer (trace_with_gradients,
-// src/integrators/gradient_domain_pt.rs:266-342), restructured into stages:
+// Streaming wavefront path tracer: PathTracer::li / render
+// (src/integrators/path_tracer.rs:59-190) and the base/offset paths of the
+// gradient-domain tracer (trace_with_gradients, gradient_domain_pt.rs:266-342),
+// restructured as the tick pipeline described in ar_engine.hpp.
 //
-//   generate -> [ extend (closest hit) -> shade (emission, NEE, BSDF sample,
-//                 Russian roulette, compaction) -> shadow (any hit) ] x max_depth
-//
-// Paths live in SoA slots; the ray and hit queues are compacted with warp
-// ballots so every stage reads contiguous 16-byte records.  Each path deposits
-// its radiance into the film exactly once, when it terminates.
+// Path state is SoA and moves with the compacted queue (double buffered), so
+// every stage reads contiguous 16-byte records; finished paths deposit L/spp
+// into their job's film exactly once and bump the job's done counter.
 #include <algorithm>
 #include <cmath>
+#include <memory>
+#include <vector>
 
+#include <cooperative_groups.h>
+
+#include "ar_engine.hpp"
 #include "ar_shading.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace ar {
 
 namespace {
 
 constexpr uint32_t kRoleBase = 0, kRoleRight = 1, kRoleDown = 2;
+constexpr uint32_t kDead = 0x80000000u;  // meta flag: slot holds no live path
 
-struct PtState {
-    // path slots
-    uint2* key;       // pixel, sample
-    float4* thr;      // throughput rgb, previous bsdf pdf
-    float4* rad;      // radiance rgb
-    uint32_t* meta;   // depth | dim << 8 | role << 24
-    // ray queues (double buffered) and hits
-    float4* ray_o[2];
-    float4* ray_d[2];
-    uint32_t* qpath[2];
+struct PathBuf {
+    float4* ray_o;  // origin, tmin
+    float4* ray_d;  // direction, tmax
+    float4* thr;    // throughput, previous bsdf pdf
+    float4* rad;    // radiance
+    uint4* key;     // job, pixel, sample, meta (depth | dim << 8 | role << 24 | dead)
+};
+
+struct Segment {
+    uint32_t job, path_offset, nsamples, roles;
+    unsigned long long sample_begin;
+};
+
+struct EngineDev {
+    JobDev* jobs;
+    const uint32_t* active;
+    const uint32_t* n_active;
+    PathBuf buf[2];
     float4* hit;
     uint32_t* hit_inst;
-    // shadow queue
     float4* sh_o;
     float4* sh_d;
-    float4* sh_c;
-    uint32_t* sh_path;  // path | kFinal
-    uint32_t* counts;   // [0..max_depth]: rays entering bounce d; [64 + d]: shadow rays of bounce d
-};
-constexpr uint32_t kFinal = 0x80000000u;
-
-struct PtParams {
-    DevScene sc;
-    CameraDev cam;
-    PtState st;
-    uint32_t width, height, spp, max_depth, rr_depth;
-    uint32_t gdpt, film64;
-    uint64_t seed;
-    uint64_t sample_begin;  // first (sample-major) path sample of this chunk
-    uint32_t chunk_samples;
-    float inv_spp;
-    void* film[3];  // PT: film[0]; GDPT: primal, dx, dy
+    float4* sh_c;   // contribution rgb, flags (bit0: final)
+    float4* sh_L;   // radiance before this bounce's NEE (final paths)
+    uint4* sh_key;  // job, pixel, role, out index
+    uint32_t* cnt;  // [0],[1]: queue length per buffer; [2]: shadow count; [3]: new paths; [4]: segments
+    Segment* plan;
+    uint32_t capacity;
+    unsigned long long* stats;  // [0] paths generated, [1] closest-hit rays, [2] shadow rays
+    int* err;
 };
 
-__device__ __forceinline__ void film_add(const PtParams& P, int which, uint32_t pix, f3 v) {
-    if (P.film64) {
-        double* f = static_cast<double*>(P.film[which]) + 3 * size_t(pix);
+__device__ __forceinline__ void film_add(const JobDev& J, int which, uint32_t pix, f3 v) {
+    if (J.film64) {
+        double* f = static_cast<double*>(J.film[which]) + 3 * size_t(pix);
         atomicAdd(f, double(v.x));
         atomicAdd(f + 1, double(v.y));
         atomicAdd(f + 2, double(v.z));
     } else {
-        float* f = static_cast<float*>(P.film[which]) + 3 * size_t(pix);
+        float* f = static_cast<float*>(J.film[which]) + 3 * size_t(pix);
         atomicAdd(f, v.x);
         atomicAdd(f + 1, v.y);
         atomicAdd(f + 2, v.z);
     }
 }
 
-// A finished path adds L/spp to its film(s).
-__device__ __forceinline__ void deposit(const PtParams& P, uint32_t p, f3 L) {
-    const uint2 k = P.st.key[p];
-    const uint32_t role = P.st.meta[p] >> 24;
-    const f3 v = L * P.inv_spp;
-    if (!P.gdpt) {
-        film_add(P, 0, k.x, v);
-        return;
-    }
-    const uint32_t px = k.x % P.width, py = k.x / P.width;
-    if (role == kRoleBase) {
-        film_add(P, 0, k.x, v);
-        if (px + 1 < P.width) film_add(P, 1, k.x, -v);
-        if (py + 1 < P.height) film_add(P, 2, k.x, -v);
-    } else {
-        film_add(P, role == kRoleRight ? 1 : 2, k.x, v);
-    }
+// Counts one finished path of `job`: lanes of the warp that finish paths of the
+// same job share one atomic.
+__device__ __forceinline__ void count_done(const EngineDev& E, uint32_t job) {
+    cg::coalesced_group g = cg::coalesced_threads();
+    cg::coalesced_group same = cg::labeled_partition(g, job);
+    if (same.thread_rank() == 0) atomicAdd(&E.jobs[job].done_paths, (unsigned long long)same.size());
 }
 
-__global__ void __launch_bounds__(256) k_generate(PtParams P) {
-    const uint32_t npix = P.width * P.height;
-    const uint32_t roles = P.gdpt ? 3u : 1u;
-    const uint32_t total = P.chunk_samples * roles;
-    for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
-        const uint32_t i = base + threadIdx.x;
-        bool live = i < total;
-        uint32_t p = i, pixel = 0, sample = 0, role = 0, px = 0, py = 0;
-        if (live) {
-            const uint32_t si = i / roles;
-            role = i - si * roles;
-            const uint64_t g = P.sample_begin + si;
-            pixel = uint32_t(g % npix);
-            sample = uint32_t(g / npix);
-            px = pixel % P.width;
-            py = pixel / P.width;
-            if (role == kRoleRight && px + 1 >= P.width) live = false;
-            if (role == kRoleDown && py + 1 >= P.height) live = false;
+// A finished path adds L/spp to its job's film(s) and counts as done.
+__device__ __forceinline__ void deposit(const EngineDev& E, uint32_t job, uint32_t pixel, uint32_t role, f3 L) {
+    JobDev& J = E.jobs[job];
+    const f3 v = L * J.inv_spp;
+    if (!J.gdpt) {
+        film_add(J, 0, pixel, v);
+    } else {
+        const uint32_t px = pixel % J.width, py = pixel / J.width;
+        if (role == kRoleBase) {
+            film_add(J, 0, pixel, v);
+            if (px + 1 < J.width) film_add(J, 1, pixel, -v);
+            if (py + 1 < J.height) film_add(J, 2, pixel, -v);
+        } else {
+            film_add(J, role == kRoleRight ? 1 : 2, pixel, v);
         }
-        const uint32_t slot = warp_alloc(&P.st.counts[0], live);
-        if (!live) continue;
-        const uint64_t key = counter_key(P.seed, pixel, sample);
+    }
+    count_done(E, job);
+}
+
+// Free slots -> samples of the active jobs, oldest first.
+__global__ void k_plan(EngineDev E, int q) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const uint32_t n_cont = E.cnt[q];
+    uint32_t used = 0, nseg = 0;
+    const uint32_t na = *E.n_active;
+    for (uint32_t a = 0; a < na && n_cont + used < E.capacity; ++a) {
+        const uint32_t j = E.active[a];
+        JobDev& J = E.jobs[j];
+        const unsigned long long rem = J.total_samples - J.next_sample;
+        if (rem == 0) continue;
+        const uint32_t free_paths = E.capacity - n_cont - used;
+        const unsigned long long take = min(rem, (unsigned long long)(free_paths / J.roles));
+        if (take == 0) break;
+        E.plan[nseg] = Segment{j, n_cont + used, uint32_t(take), J.roles, J.next_sample};
+        J.next_sample += take;
+        used += uint32_t(take) * J.roles;
+        nseg++;
+    }
+    E.cnt[3] = used;
+    E.cnt[4] = nseg;
+    E.cnt[q] = n_cont + used;
+    E.cnt[q ^ 1] = 0;
+    E.cnt[2] = 0;
+    E.stats[0] += used;
+}
+
+__global__ void __launch_bounds__(256) k_generate(EngineDev E, int q) {
+    const uint32_t n_new = E.cnt[3], nseg = E.cnt[4];
+    const uint32_t base_off = E.cnt[q] - n_new;
+    const PathBuf B = E.buf[q];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_new; i += gridDim.x * blockDim.x) {
+        const uint32_t k = base_off + i;
+        uint32_t lo = 0, hi = nseg;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (E.plan[mid].path_offset <= k) lo = mid; else hi = mid;
+        }
+        const Segment sg = E.plan[lo];
+        const JobDev& J = E.jobs[sg.job];
+        const uint32_t rel = k - sg.path_offset;
+        const uint32_t si = rel / sg.roles, role = rel - si * sg.roles;
+        const unsigned long long g = sg.sample_begin + si;
+        const uint32_t npix = J.width * J.height;
+        const uint32_t pixel = uint32_t(g % npix), sample = uint32_t(g / npix);
+        const uint32_t px = pixel % J.width, py = pixel / J.width;
+        const bool skip = (role == kRoleRight && px + 1 >= J.width) || (role == kRoleDown && py + 1 >= J.height);
+        if (skip) {
+            // Offset path outside the image: zero gradient, no trace (gdpt.rs:298-327).
+            B.key[k] = make_uint4(sg.job, pixel, sample, kDead | (role << 24));
+            count_done(E, sg.job);
+            continue;
+        }
+        const uint64_t key = counter_key(J.seed, pixel, sample);
         const float jx = counter_u01(key, 0), jy = counter_u01(key, 1);
         const uint32_t ox = px + (role == kRoleRight ? 1u : 0u), oy = py + (role == kRoleDown ? 1u : 0u);
-        const float u = (float(ox) + jx) / float(P.width);
-        const float v = 1.0f - (float(oy) + jy) / float(P.height);
-        const Ray r = camera_ray(P.cam, u, v);
-        P.st.key[p] = make_uint2(pixel, sample);
-        P.st.thr[p] = make_float4(1.f, 1.f, 1.f, 0.f);
-        P.st.rad[p] = make_float4(0.f, 0.f, 0.f, 0.f);
-        P.st.meta[p] = (2u << 8) | (role << 24);
-        P.st.ray_o[0][slot] = make_float4(r.o.x, r.o.y, r.o.z, r.tmin);
-        P.st.ray_d[0][slot] = make_float4(r.d.x, r.d.y, r.d.z, r.tmax);
-        P.st.qpath[0][slot] = p;
+        const Ray r = camera_ray(J.cam, (float(ox) + jx) / float(J.width), 1.0f - (float(oy) + jy) / float(J.height));
+        B.ray_o[k] = make_float4(r.o.x, r.o.y, r.o.z, r.tmin);
+        B.ray_d[k] = make_float4(r.d.x, r.d.y, r.d.z, r.tmax);
+        B.thr[k] = make_float4(1.f, 1.f, 1.f, 0.f);
+        B.rad[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+        B.key[k] = make_uint4(sg.job, pixel, sample, (2u << 8) | (role << 24));
     }
 }
 
-__global__ void __launch_bounds__(128) k_extend(PtParams P, uint32_t depth, int* err) {
-    const uint32_t n = P.st.counts[depth];
-    const int q = depth & 1;
+__global__ void __launch_bounds__(128) k_extend(EngineDev E, int q) {
+    const uint32_t n = E.cnt[q];
+    const PathBuf B = E.buf[q];
+    if (blockIdx.x == 0 && threadIdx.x == 0) E.stats[1] += n;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-        const float4 a = P.st.ray_o[q][j], b = P.st.ray_d[q][j];
-        const Ray r{mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w};
+        const uint4 kk = B.key[j];
         HitRec h;
-        traverse<false>(P.sc, r, h, err);
-        P.st.hit[j] = make_float4(h.t, h.u, h.v, __uint_as_float(h.slot));
-        P.st.hit_inst[j] = h.inst;
+        h.slot = kInvalid;
+        h.inst = kInvalid;
+        h.t = h.u = h.v = 0.f;
+        if (!(kk.w & kDead)) {
+            const float4 a = B.ray_o[j], b = B.ray_d[j];
+            traverse<false>(E.jobs[kk.x].sc, Ray{mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w}, h, E.err);
+        }
+        E.hit[j] = make_float4(h.t, h.u, h.v, __uint_as_float(h.slot));
+        E.hit_inst[j] = h.inst;
     }
 }
 
-__global__ void __launch_bounds__(256) k_shade(PtParams P, uint32_t depth) {
-    const uint32_t n = P.st.counts[depth];
-    const int q = depth & 1;
-    uint32_t* out_count = &P.st.counts[depth + 1];
-    uint32_t* sh_count = &P.st.counts[64 + depth];
+__global__ void __launch_bounds__(256) k_shade(EngineDev E, int q) {
+    const uint32_t n = E.cnt[q];
+    const PathBuf B = E.buf[q], O = E.buf[q ^ 1];
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
         const uint32_t j = base + threadIdx.x;
-        const bool active = j < n;
-        bool cont = false, shadow = false;
-        uint32_t p = 0;
-        f3 new_o, new_d, sh_o, sh_d, sh_c;
-        float sh_tmax = 0.f;
-        f3 L, thr;
-        float prev_pdf = 0.f;
-        uint32_t meta = 0;
-        if (active) {
-            p = P.st.qpath[q][j];
-            const float4 h = P.st.hit[j];
-            const float4 t4 = P.st.thr[p], r4 = P.st.rad[p];
+        bool cont = false, shadow = false, live = false;
+        uint4 kk = make_uint4(0, 0, 0, 0);
+        f3 new_o, new_d, sh_o, sh_d, sh_c, L, thr;
+        float sh_tmax = 0.f, prev_pdf = 0.f;
+        if (j < n) {
+            kk = B.key[j];
+            live = !(kk.w & kDead);
+        }
+        if (live) {
+            const JobDev& J = E.jobs[kk.x];
+            const float4 h = E.hit[j];
+            const float4 t4 = B.thr[j], r4 = B.rad[j];
             thr = mk(t4.x, t4.y, t4.z);
             prev_pdf = t4.w;
             L = mk(r4.x, r4.y, r4.z);
-            meta = P.st.meta[p];
+            const uint32_t depth = kk.w & 0xffu;
+            uint32_t dim = (kk.w >> 8) & 0xffffu;
             const uint32_t slot = __float_as_uint(h.w);
             if (slot != kInvalid) {
-                const uint2 k = P.st.key[p];
-                const uint64_t key = counter_key(P.seed, k.x, k.y);
-                uint32_t dim = (meta >> 8) & 0xffffu;
-                const float4 ro4 = P.st.ray_o[q][j], rd4 = P.st.ray_d[q][j];
+                const DevScene& sc = J.sc;
+                const uint64_t key = counter_key(J.seed, kk.y, kk.z);
+                const float4 ro4 = B.ray_o[j], rd4 = B.ray_d[j];
                 const f3 ro = mk(ro4.x, ro4.y, ro4.z), rd = mk(rd4.x, rd4.y, rd4.z);
-                const Shade s = make_shade(P.sc, ro, rd, h.x, h.y, h.z, slot, P.st.hit_inst[j]);
-                const MatView m = load_mat(P.sc, s.mat);
+                const Shade s = make_shade(sc, ro, rd, h.x, h.y, h.z, slot, E.hit_inst[j]);
+                const MatView m = load_mat(sc, s.mat);
                 const f3 wo = -rd;
                 const f3 wo_l = to_local(s.onb, wo);
-                const bool lights_on = light_enabled(P.sc);
+                const bool lights_on = light_enabled(sc);
                 // Emission on hit (area-light extension).
                 if (m.emitter >= 0) {
-                    const LightView lt = load_light(P.sc, uint32_t(m.emitter));
+                    const LightView lt = load_light(sc, uint32_t(m.emitter));
                     const float cos_l = dot(lt.n, wo);
                     if (cos_l > 0.f) {
                         if (depth == 0 || !lights_on) {
                             L = L + thr * lt.inten;
                         } else {
                             const float pdf_light =
-                                light_pmf_of(P.sc, uint32_t(m.emitter)) * (h.x * h.x) / (cos_l * lt.area);
-                            const float w = power_heuristic(prev_pdf, pdf_light);
-                            L = L + (thr * lt.inten) * w;
+                                light_pmf_of(sc, uint32_t(m.emitter)) * (h.x * h.x) / (cos_l * lt.area);
+                            L = L + (thr * lt.inten) * power_heuristic(prev_pdf, pdf_light);
                         }
                     }
                 }
-                // Next-event estimation: one light, one shadow ray.
+                // Next-event estimation (path_tracer.rs:79-117).
                 if (lights_on) {
                     const float u_sel = counter_u01(key, dim++);
                     const float ulx = counter_u01(key, dim++);
                     const float uly = counter_u01(key, dim++);
                     uint32_t li;
                     float sel;
-                    light_select(P.sc, u_sel, li, sel);
-                    const LightView light = load_light(P.sc, li);
+                    light_select(sc, u_sel, li, sel);
+                    const LightView light = load_light(sc, li);
                     f3 wi, lrad;
                     float dist, lpdf;
                     if (light_sample(light, s.p, ulx, uly, wi, dist, lrad, lpdf)) {
@@ -211,8 +254,7 @@ __global__ void __launch_bounds__(256) k_shade(PtParams P, uint32_t depth) {
                                 c = ((((thr * f) * cos_wi) * lrad) * w) / pdf_light;
                             }
                             if (!is_zero(c)) {
-                                const f3 off = (s.n * 1e-4f) * signum(dot(wi, s.n));
-                                sh_o = s.p + off;
+                                sh_o = s.p + (s.n * 1e-4f) * signum(dot(wi, s.n));
                                 sh_d = normalize(wi);
                                 sh_tmax = dist * (1.0f - 1e-4f);
                                 sh_c = c;
@@ -221,93 +263,77 @@ __global__ void __launch_bounds__(256) k_shade(PtParams P, uint32_t depth) {
                         }
                     }
                 }
-                // BSDF sampling, Russian roulette, spawn.
-                const float u_bsel = counter_u01(key, dim++);
-                (void)u_bsel;
+                // BSDF sampling, Russian roulette, spawn (:119-153).
+                dim++;  // u_sel of Bsdf::sample (unused by these BSDFs)
                 const float udx = counter_u01(key, dim++);
                 const float udy = counter_u01(key, dim++);
                 f3 wi, f;
                 float pdf;
                 if (bsdf_sample(m, wo_l, udx, udy, wi, pdf, f) && pdf != 0.f && !is_zero(f)) {
-                    const float cos_wi = fabsf(wi.z);
-                    thr = thr * ((f * cos_wi) / pdf);
+                    thr = thr * ((f * fabsf(wi.z)) / pdf);
                     prev_pdf = pdf;
                     bool alive = true;
-                    if (depth + 1 >= P.rr_depth) {
+                    if (depth + 1 >= J.rr_depth) {
                         const float survival = fminf(max3(thr), 0.95f);
                         if (counter_u01(key, dim++) > survival) alive = false;
                         else thr = thr / survival;
                     }
-                    if (alive && depth + 1 < P.max_depth) {
+                    if (alive && depth + 1 < J.max_depth) {
                         const f3 wi_w = to_world(s.onb, wi);
-                        const f3 off = (s.n * 1e-4f) * signum(dot(wi_w, s.n));
-                        new_o = s.p + off;
+                        new_o = s.p + (s.n * 1e-4f) * signum(dot(wi_w, s.n));
                         new_d = normalize(wi_w);
                         cont = true;
                     }
                 }
-                meta = (meta & 0xff000000u) | (dim << 8) | (depth + 1);
+                kk.w = (kk.w & 0xff000000u) | (dim << 8) | (depth + 1);
             }
         }
-        const uint32_t rs = warp_alloc(out_count, cont);
-        const uint32_t ss = warp_alloc(sh_count, shadow);
-        if (!active) continue;
+        const uint32_t rs = warp_alloc(&E.cnt[q ^ 1], cont);
+        const uint32_t ss = warp_alloc(&E.cnt[2], shadow);
+        if (!live) continue;
         if (cont) {
-            P.st.ray_o[q ^ 1][rs] = make_float4(new_o.x, new_o.y, new_o.z, 1e-4f);
-            P.st.ray_d[q ^ 1][rs] = make_float4(new_d.x, new_d.y, new_d.z, FLT_MAX);
-            P.st.qpath[q ^ 1][rs] = p;
-            P.st.thr[p] = make_float4(thr.x, thr.y, thr.z, prev_pdf);
-            P.st.meta[p] = meta;
+            O.ray_o[rs] = make_float4(new_o.x, new_o.y, new_o.z, 1e-4f);
+            O.ray_d[rs] = make_float4(new_d.x, new_d.y, new_d.z, FLT_MAX);
+            O.thr[rs] = make_float4(thr.x, thr.y, thr.z, prev_pdf);
+            O.rad[rs] = make_float4(L.x, L.y, L.z, 0.f);
+            O.key[rs] = kk;
         }
+        const uint32_t role = (kk.w >> 24) & 3u;
         if (shadow) {
-            P.st.sh_o[ss] = make_float4(sh_o.x, sh_o.y, sh_o.z, 0.f);
-            P.st.sh_d[ss] = make_float4(sh_d.x, sh_d.y, sh_d.z, sh_tmax);
-            P.st.sh_c[ss] = make_float4(sh_c.x, sh_c.y, sh_c.z, 0.f);
-            P.st.sh_path[ss] = p | (cont ? 0u : kFinal);
-        }
-        if (cont || shadow) {
-            P.st.rad[p] = make_float4(L.x, L.y, L.z, 0.f);
-        } else {
-            deposit(P, p, L);
+            E.sh_o[ss] = make_float4(sh_o.x, sh_o.y, sh_o.z, 0.f);
+            E.sh_d[ss] = make_float4(sh_d.x, sh_d.y, sh_d.z, sh_tmax);
+            E.sh_c[ss] = make_float4(sh_c.x, sh_c.y, sh_c.z, __uint_as_float(cont ? 0u : 1u));
+            E.sh_L[ss] = make_float4(L.x, L.y, L.z, 0.f);
+            E.sh_key[ss] = make_uint4(kk.x, kk.y, role, rs);
+        } else if (!cont) {
+            deposit(E, kk.x, kk.y, role, L);
         }
     }
 }
 
-__global__ void __launch_bounds__(128) k_shadow(PtParams P, uint32_t depth, int* err) {
-    const uint32_t n = P.st.counts[64 + depth];
+__global__ void __launch_bounds__(128) k_shadow(EngineDev E, int q) {
+    const uint32_t n = E.cnt[2];
+    const PathBuf O = E.buf[q ^ 1];
+    if (blockIdx.x == 0 && threadIdx.x == 0) E.stats[2] += n;
     for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
-        const float4 a = P.st.sh_o[m], b = P.st.sh_d[m];
-        const Ray r{mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w};
+        const float4 a = E.sh_o[m], b = E.sh_d[m];
+        const uint4 sk = E.sh_key[m];
         HitRec h;
-        traverse<true>(P.sc, r, h, err);
-        const uint32_t e = P.st.sh_path[m];
-        const uint32_t p = e & ~kFinal;
-        const float4 r4 = P.st.rad[p];
-        f3 L = mk(r4.x, r4.y, r4.z);
-        if (h.slot == kInvalid) {
-            const float4 c = P.st.sh_c[m];
-            L = L + mk(c.x, c.y, c.z);
+        traverse<true>(E.jobs[sk.x].sc, Ray{mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w}, h, E.err);
+        const float4 c = E.sh_c[m];
+        const bool visible = h.slot == kInvalid;
+        if (__float_as_uint(c.w) & 1u) {
+            const float4 l = E.sh_L[m];
+            f3 L = mk(l.x, l.y, l.z);
+            if (visible) L = L + mk(c.x, c.y, c.z);
+            deposit(E, sk.x, sk.y, sk.z, L);
+        } else if (visible) {
+            float4 r = O.rad[sk.w];
+            r.x += c.x;
+            r.y += c.y;
+            r.z += c.z;
+            O.rad[sk.w] = r;
         }
-        if (e & kFinal) deposit(P, p, L);
-        else P.st.rad[p] = make_float4(L.x, L.y, L.z, 0.f);
-    }
-}
-
-// Folds one chunk's queue counters into the context's 64-bit work counters:
-// [0] paths, [1] closest-hit rays, [2] shadow rays.
-__global__ void k_count(const uint32_t* counts, uint32_t max_depth, unsigned long long* stats) {
-    __shared__ unsigned long long ext, sh;
-    if (threadIdx.x == 0) { ext = 0; sh = 0; }
-    __syncthreads();
-    if (threadIdx.x < max_depth) {
-        atomicAdd(&ext, (unsigned long long)counts[threadIdx.x]);
-        atomicAdd(&sh, (unsigned long long)counts[64 + threadIdx.x]);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        stats[0] += counts[0];
-        stats[1] += ext;
-        stats[2] += sh;
     }
 }
 
@@ -321,93 +347,258 @@ T* carve(char*& cur, size_t n) {
 
 }  // namespace
 
+struct PathEngine {
+    ar_context* ctx = nullptr;
+    uint32_t cap = 0;
+    DevBuf mem, jobs_d, active_d;
+    EngineDev E{};
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaStream_t captured_stream = nullptr;
+    int parity = 0;
+    uint64_t ticks = 0;
+    std::vector<uint32_t> active;
+    unsigned long long* done_h = nullptr;
+    // Pinned staging for job-table updates, two halves used alternately; each
+    // half is reused only after the event of its last copy has completed.
+    struct Staging {
+        JobDev* jobs = nullptr;
+        uint32_t* active = nullptr;
+        cudaEvent_t ev = nullptr;
+    } stage[2];
+    int stage_next = 0;
+
+    void launch_tick(int q, cudaStream_t s) {
+        const int wide = ctx->num_sms * 8;
+        k_plan<<<1, 32, 0, s>>>(E, q);
+        k_generate<<<wide, 256, 0, s>>>(E, q);
+        k_extend<<<ctx->num_sms * 16, 128, 0, s>>>(E, q);
+        k_shade<<<wide, 256, 0, s>>>(E, q);
+        k_shadow<<<ctx->num_sms * 16, 128, 0, s>>>(E, q);
+    }
+
+    void build_graphs() {
+        for (int q = 0; q < 2; ++q) {
+            if (graph[q]) cudaGraphExecDestroy(graph[q]);
+            graph[q] = nullptr;
+        }
+        cudaStream_t s = ctx->stream;
+        for (int q = 0; q < 2; ++q) {
+            cudaGraph_t g;
+            AR_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            launch_tick(q, s);
+            AR_CUDA(cudaStreamEndCapture(s, &g));
+            AR_CUDA(cudaGraphInstantiate(&graph[q], g, 0));
+            cudaGraphDestroy(g);
+        }
+        captured_stream = s;
+    }
+
+    ~PathEngine() {
+        for (int q = 0; q < 2; ++q)
+            if (graph[q]) cudaGraphExecDestroy(graph[q]);
+        if (done_h) cudaFreeHost(done_h);
+        for (auto& s : stage) {
+            if (s.jobs) cudaFreeHost(s.jobs);
+            if (s.active) cudaFreeHost(s.active);
+            if (s.ev) cudaEventDestroy(s.ev);
+        }
+    }
+};
+
+PathEngine* engine_create(ar_context* ctx, uint32_t capacity) {
+    auto e = std::make_unique<PathEngine>();
+    e->ctx = ctx;
+    e->cap = capacity;
+    const size_t c = capacity;
+    size_t bytes = 2 * c * (4 * sizeof(float4) + sizeof(uint4)) + c * (sizeof(float4) + sizeof(uint32_t)) +
+                   c * (4 * sizeof(float4) + sizeof(uint4)) + 64 * sizeof(uint32_t) +
+                   kMaxActiveJobs * sizeof(Segment) + 8 * sizeof(unsigned long long) + 32 * 256;
+    e->mem.alloc(bytes);
+    char* cur = e->mem.as<char>();
+    for (int b = 0; b < 2; ++b) {
+        e->E.buf[b].ray_o = carve<float4>(cur, c);
+        e->E.buf[b].ray_d = carve<float4>(cur, c);
+        e->E.buf[b].thr = carve<float4>(cur, c);
+        e->E.buf[b].rad = carve<float4>(cur, c);
+        e->E.buf[b].key = carve<uint4>(cur, c);
+    }
+    e->E.hit = carve<float4>(cur, c);
+    e->E.hit_inst = carve<uint32_t>(cur, c);
+    e->E.sh_o = carve<float4>(cur, c);
+    e->E.sh_d = carve<float4>(cur, c);
+    e->E.sh_c = carve<float4>(cur, c);
+    e->E.sh_L = carve<float4>(cur, c);
+    e->E.sh_key = carve<uint4>(cur, c);
+    e->E.cnt = carve<uint32_t>(cur, 64);
+    e->E.plan = carve<Segment>(cur, kMaxActiveJobs);
+    e->E.stats = carve<unsigned long long>(cur, 8);
+    e->E.capacity = capacity;
+    e->E.err = ctx->err_flag.as<int>();
+    e->jobs_d.alloc(kMaxActiveJobs * sizeof(JobDev));
+    e->active_d.alloc((kMaxActiveJobs + 1) * sizeof(uint32_t));
+    e->E.jobs = e->jobs_d.as<JobDev>();
+    e->E.active = e->active_d.as<uint32_t>();
+    e->E.n_active = e->active_d.as<uint32_t>() + kMaxActiveJobs;
+    AR_CUDA(cudaMemsetAsync(e->E.cnt, 0, 64 * sizeof(uint32_t), ctx->stream));
+    AR_CUDA(cudaMemsetAsync(e->E.stats, 0, 8 * sizeof(unsigned long long), ctx->stream));
+    AR_CUDA(cudaMemsetAsync(e->active_d.ptr, 0, (kMaxActiveJobs + 1) * sizeof(uint32_t), ctx->stream));
+    AR_CUDA(cudaMallocHost(&e->done_h, kMaxActiveJobs * sizeof(unsigned long long)));
+    for (auto& s : e->stage) {
+        AR_CUDA(cudaMallocHost(&s.jobs, kMaxActiveJobs * sizeof(JobDev)));
+        AR_CUDA(cudaMallocHost(&s.active, (kMaxActiveJobs + 1) * sizeof(uint32_t)));
+        AR_CUDA(cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming));
+        AR_CUDA(cudaEventRecord(s.ev, ctx->stream));
+    }
+    e->build_graphs();
+    return e.release();
+}
+
+void engine_destroy(PathEngine* e) { delete e; }
+
+void engine_update(PathEngine* e, const std::vector<std::pair<uint32_t, JobDev>>& adds,
+                   const std::vector<uint32_t>& removes) {
+    if (adds.empty() && removes.empty()) return;
+    for (uint32_t slot : removes) {
+        auto it = std::find(e->active.begin(), e->active.end(), slot);
+        if (it != e->active.end()) e->active.erase(it);
+    }
+    AR_REQUIRE(e->active.size() + adds.size() <= kMaxActiveJobs, AR_ERR_REJECTED, "too many active jobs");
+    auto& st = e->stage[e->stage_next];
+    e->stage_next ^= 1;
+    AR_CUDA(cudaEventSynchronize(st.ev));  // its previous copies have been consumed
+    for (size_t i = 0; i < adds.size(); ++i) {
+        const uint32_t slot = adds[i].first;
+        AR_REQUIRE(slot < kMaxActiveJobs, AR_ERR_INVALID_ARGUMENT, "job slot out of range");
+        st.jobs[i] = adds[i].second;
+        AR_CUDA(cudaMemcpyAsync(e->E.jobs + slot, &st.jobs[i], sizeof(JobDev), cudaMemcpyHostToDevice,
+                                e->ctx->stream));
+        e->active.push_back(slot);
+    }
+    for (size_t i = 0; i < e->active.size(); ++i) st.active[i] = e->active[i];
+    st.active[kMaxActiveJobs] = uint32_t(e->active.size());
+    if (!e->active.empty())
+        AR_CUDA(cudaMemcpyAsync(e->active_d.ptr, st.active, e->active.size() * sizeof(uint32_t),
+                                cudaMemcpyHostToDevice, e->ctx->stream));
+    AR_CUDA(cudaMemcpyAsync(e->active_d.as<uint32_t>() + kMaxActiveJobs, st.active + kMaxActiveJobs,
+                            sizeof(uint32_t), cudaMemcpyHostToDevice, e->ctx->stream));
+    AR_CUDA(cudaEventRecord(st.ev, e->ctx->stream));
+}
+
+void engine_add_job(PathEngine* e, uint32_t slot, const JobDev& job) { engine_update(e, {{slot, job}}, {}); }
+
+void engine_remove_job(PathEngine* e, uint32_t slot) { engine_update(e, {}, {slot}); }
+
+void engine_tick(PathEngine* e) {
+    ar_context* ctx = e->ctx;
+    const int q = e->parity;
+    if (ctx->prof.on) {
+        // Profiling: launch the stages individually, each bracketed by events.
+        cudaStream_t s = ctx->stream;
+        const int wide = ctx->num_sms * 8;
+        { KernelScope k(ctx->prof, s, "pt_plan"); k_plan<<<1, 32, 0, s>>>(e->E, q); }
+        { KernelScope k(ctx->prof, s, "pt_generate"); k_generate<<<wide, 256, 0, s>>>(e->E, q); }
+        { KernelScope k(ctx->prof, s, "pt_extend"); k_extend<<<ctx->num_sms * 16, 128, 0, s>>>(e->E, q); }
+        { KernelScope k(ctx->prof, s, "pt_shade"); k_shade<<<wide, 256, 0, s>>>(e->E, q); }
+        { KernelScope k(ctx->prof, s, "pt_shadow"); k_shadow<<<ctx->num_sms * 16, 128, 0, s>>>(e->E, q); }
+        AR_CUDA(cudaGetLastError());
+    } else {
+        if (e->captured_stream != ctx->stream) e->build_graphs();
+        AR_CUDA(cudaGraphLaunch(e->graph[q], ctx->stream));
+    }
+    e->parity ^= 1;
+    e->ticks++;
+}
+
+const unsigned long long* engine_snapshot_done(PathEngine* e) {
+    // done_paths lives at a fixed offset inside each JobDev: gather with one
+    // strided 2D copy.
+    const size_t off = offsetof(JobDev, done_paths);
+    AR_CUDA(cudaMemcpy2DAsync(e->done_h, sizeof(unsigned long long), reinterpret_cast<char*>(e->E.jobs) + off,
+                              sizeof(JobDev), sizeof(unsigned long long), kMaxActiveJobs, cudaMemcpyDeviceToHost,
+                              e->ctx->stream));
+    return e->done_h;
+}
+
+const unsigned long long* engine_snapshot_host(const PathEngine* e) { return e->done_h; }
+
+uint64_t engine_ticks(const PathEngine* e) { return e->ticks; }
+uint32_t engine_capacity(const PathEngine* e) { return e->cap; }
+bool engine_has_active(const PathEngine* e) { return !e->active.empty(); }
+
+void engine_stats(PathEngine* e, unsigned long long* out3_pinned) {
+    AR_CUDA(cudaMemcpyAsync(out3_pinned, e->E.stats, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                            e->ctx->stream));
+}
+
+// Single-job render through the engine (Integrator::render for PT / GDPT
+// paths): the "plain" one-job-at-a-time path.
 void render_pt_films(ar_context* ctx, const ar_scene* sc, const CameraDev& cam, const ar_integrator_cfg& cfg,
                      uint32_t w, uint32_t h, bool gdpt, void* films) {
-    AR_REQUIRE(cfg.max_depth <= 63, AR_ERR_INVALID_ARGUMENT, "max_depth must be <= 63");
-    const uint64_t total = uint64_t(w) * h * cfg.spp;
+    AR_REQUIRE(cfg.max_depth <= 255, AR_ERR_INVALID_ARGUMENT, "max_depth must be <= 255");
+    if (!ctx->engine) ctx->engine = engine_create(ctx, ctx->engine_capacity);
+    PathEngine* e = ctx->engine;
     const uint32_t roles = gdpt ? 3u : 1u;
-    // Path capacity: up to 2M path slots per chunk.
-    const uint32_t cap_paths = 1u << 21;
-    const uint32_t chunk = uint32_t(std::min<uint64_t>(total, cap_paths / roles));
-    const uint32_t cap = chunk * roles;
-    size_t bytes = 0;
-    bytes += cap * (sizeof(uint2) + 2 * sizeof(float4) + sizeof(uint32_t));
-    bytes += 2 * cap * (2 * sizeof(float4) + sizeof(uint32_t));
-    bytes += cap * (sizeof(float4) + sizeof(uint32_t));
-    bytes += cap * (3 * sizeof(float4) + sizeof(uint32_t));
-    bytes += 128 * sizeof(uint32_t) + 32 * 256;
-    ctx->work.ensure(bytes);
-    char* cur = ctx->work.buf.as<char>();
-    PtParams P{};
-    P.sc = sc->view;
-    P.cam = cam;
-    P.st.key = carve<uint2>(cur, cap);
-    P.st.thr = carve<float4>(cur, cap);
-    P.st.rad = carve<float4>(cur, cap);
-    P.st.meta = carve<uint32_t>(cur, cap);
-    for (int b = 0; b < 2; ++b) {
-        P.st.ray_o[b] = carve<float4>(cur, cap);
-        P.st.ray_d[b] = carve<float4>(cur, cap);
-        P.st.qpath[b] = carve<uint32_t>(cur, cap);
-    }
-    P.st.hit = carve<float4>(cur, cap);
-    P.st.hit_inst = carve<uint32_t>(cur, cap);
-    P.st.sh_o = carve<float4>(cur, cap);
-    P.st.sh_d = carve<float4>(cur, cap);
-    P.st.sh_c = carve<float4>(cur, cap);
-    P.st.sh_path = carve<uint32_t>(cur, cap);
-    P.st.counts = carve<uint32_t>(cur, 128);
-    P.width = w;
-    P.height = h;
-    P.spp = cfg.spp;
-    P.max_depth = cfg.max_depth;
-    P.rr_depth = cfg.rr_depth;
-    P.gdpt = gdpt ? 1u : 0u;
-    P.film64 = cfg.film_precision == AR_FILM_F64 ? 1u : 0u;
-    P.seed = cfg.seed;
-    P.inv_spp = 1.0f / float(cfg.spp);
-    const size_t film_bytes = size_t(w) * h * 3 * (P.film64 ? sizeof(double) : sizeof(float));
-    for (int f = 0; f < int(roles); ++f) {
-        P.film[f] = static_cast<char*>(films) + f * film_bytes;
-    }
+    const bool f64 = cfg.film_precision == AR_FILM_F64;
+    const size_t film_bytes = size_t(w) * h * 3 * (f64 ? sizeof(double) : sizeof(float));
     AR_CUDA(cudaMemsetAsync(films, 0, film_bytes * roles, ctx->stream));
-    AR_CUDA(cudaMemsetAsync(ctx->stats_d.ptr, 0, 8 * sizeof(uint64_t), ctx->stream));
-    const int grid_wide = ctx->num_sms * 8;
-    int* err = ctx->err_flag.as<int>();
-    uint64_t chunks = 0;
-    for (uint64_t begin = 0; begin < total; begin += chunk, ++chunks) {
-        P.sample_begin = begin;
-        P.chunk_samples = uint32_t(std::min<uint64_t>(chunk, total - begin));
-        AR_CUDA(cudaMemsetAsync(P.st.counts, 0, 128 * sizeof(uint32_t), ctx->stream));
-        const int gen_grid = int(std::min<uint64_t>((uint64_t(P.chunk_samples) * roles + 255) / 256, grid_wide));
-        {
-            KernelScope ks(ctx->prof, ctx->stream, "pt_generate");
-            k_generate<<<std::max(1, gen_grid), 256, 0, ctx->stream>>>(P);
+    JobDev J{};
+    J.sc = sc->view;
+    J.cam = cam;
+    J.width = w;
+    J.height = h;
+    J.spp = cfg.spp;
+    J.max_depth = cfg.max_depth;
+    J.rr_depth = cfg.rr_depth;
+    J.gdpt = gdpt ? 1u : 0u;
+    J.film64 = f64 ? 1u : 0u;
+    J.roles = roles;
+    J.seed = cfg.seed;
+    J.inv_spp = 1.0f / float(cfg.spp);
+    for (uint32_t f = 0; f < roles; ++f) J.film[f] = static_cast<char*>(films) + f * film_bytes;
+    J.total_samples = uint64_t(w) * h * cfg.spp;
+    J.total_paths = J.total_samples * roles;
+    J.next_sample = 0;
+    J.done_paths = 0;
+    const uint32_t slot = 0;
+    unsigned long long before[3];
+    AR_CUDA(cudaMemcpyAsync(before, e->E.stats, sizeof(before), cudaMemcpyDeviceToHost, ctx->stream));
+    engine_add_job(e, slot, J);  // synchronises the stream once
+    // Tick until every path has deposited; completion is checked one tick behind
+    // so the GPU always has the next tick queued.
+    cudaEvent_t ev[2];
+    AR_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+    AR_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+    unsigned long long* done_pinned = e->done_h;  // two entries, one per in-flight tick
+    uint64_t issued = 0;
+    const uint64_t tick_cap = 1ull << 26;
+    bool done = false;
+    while (!done) {
+        engine_tick(e);
+        const int cur = int(issued & 1);
+        AR_CUDA(cudaMemcpyAsync(done_pinned + cur, &e->E.jobs[slot].done_paths, sizeof(unsigned long long),
+                                cudaMemcpyDeviceToHost, ctx->stream));
+        AR_CUDA(cudaEventRecord(ev[cur], ctx->stream));
+        issued++;
+        if (issued >= 2) {
+            const int prev = int((issued - 2) & 1);  // the tick before the one just queued
+            AR_CUDA(cudaEventSynchronize(ev[prev]));
+            if (done_pinned[prev] >= J.total_paths) done = true;
         }
-        for (uint32_t d = 0; d < cfg.max_depth; ++d) {
-            {
-                KernelScope ks(ctx->prof, ctx->stream, "pt_extend");
-                k_extend<<<ctx->num_sms * 16, 128, 0, ctx->stream>>>(P, d, err);
-            }
-            {
-                KernelScope ks(ctx->prof, ctx->stream, "pt_shade");
-                k_shade<<<grid_wide, 256, 0, ctx->stream>>>(P, d);
-            }
-            {
-                KernelScope ks(ctx->prof, ctx->stream, "pt_shadow");
-                k_shadow<<<ctx->num_sms * 16, 128, 0, ctx->stream>>>(P, d, err);
-            }
-        }
-        k_count<<<1, 64, 0, ctx->stream>>>(P.st.counts, cfg.max_depth, ctx->stats_d.as<unsigned long long>());
-        AR_CUDA(cudaGetLastError());
+        AR_REQUIRE(issued < tick_cap, AR_ERR_TIMEOUT, "render did not converge");
     }
-    // Counters land in pinned memory; ar_get_render_stats reads them after a sync.
-    AR_CUDA(cudaMemcpyAsync(ctx->stats_h, ctx->stats_d.ptr, 8 * sizeof(uint64_t), cudaMemcpyDeviceToHost,
-                            ctx->stream));
-    ctx->stats_pending = true;
-    ctx->last_stats.path_samples = total;
-    ctx->last_stats.extend_launches = chunks * cfg.max_depth;
-    ctx->last_stats.shadow_launches = chunks * cfg.max_depth;
+    AR_CUDA(cudaStreamSynchronize(ctx->stream));
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    engine_remove_job(e, slot);
+    unsigned long long after[3];
+    AR_CUDA(cudaMemcpy(after, e->E.stats, sizeof(after), cudaMemcpyDeviceToHost));
+    ctx->last_stats.path_samples = J.total_samples;
+    ctx->last_stats.paths = after[0] - before[0];
+    ctx->last_stats.extend_rays = after[1] - before[1];
+    ctx->last_stats.shadow_rays = after[2] - before[2];
+    ctx->last_stats.extend_launches = issued;
+    ctx->last_stats.shadow_launches = issued;
+    ctx->stats_pending = false;
 }
 
 }  // namespace ar

@@ -1,0 +1,548 @@
+// Render server: continuous batching of render jobs into shared wavefront
+// kernels (ar_server_* / ar_job_* in include/agentray.h).
+//
+// One worker thread owns two internal contexts (streams) on the device:
+//   * the PT stream runs the streaming path engine (PT and GDPT jobs); every
+//     admitted job's samples flow into the same path pool, oldest job first;
+//   * the BDPT stream runs sample batches that mix every active BDPT job.
+// Admission is FIFO under an HBM budget for job films; completion is detected
+// from pinned snapshots of the per-job done counters (PT) or batch events
+// (BDPT), then the film is converted (GDPT: Poisson-reconstructed) and copied
+// to the caller's host buffer before the job reports DONE.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "ar_bdpt.hpp"
+#include "ar_engine.hpp"
+
+namespace ar {
+
+ar_context* context_create_internal(int device);
+void context_destroy_internal(ar_context* ctx);
+
+namespace {
+
+// Size-class cache of device buffers (job films and staging), so admission
+// does not call cudaMalloc on the hot path.
+class DevicePool {
+  public:
+    void* get(size_t bytes) {
+        bytes = round(bytes);
+        auto& v = free_[bytes];
+        if (!v.empty()) {
+            void* p = v.back();
+            v.pop_back();
+            return p;
+        }
+        void* p = nullptr;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess)
+            throw ArError{AR_ERR_OUT_OF_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e)};
+        return p;
+    }
+    void put(void* p, size_t bytes) {
+        if (p) free_[round(bytes)].push_back(p);
+    }
+    ~DevicePool() {
+        for (auto& kv : free_)
+            for (void* p : kv.second) cudaFree(p);
+    }
+    static size_t round(size_t b) { return (b + (1u << 20) - 1) & ~size_t((1u << 20) - 1); }
+
+  private:
+    std::map<size_t, std::vector<void*>> free_;
+};
+
+enum class Kind { PathTraced, Bidirectional };
+
+struct SJob {
+    uint64_t id = 0;
+    const ar_scene* scene = nullptr;
+    ar_camera_desc cam{};
+    ar_integrator_cfg cfg{};
+    uint32_t w = 0, h = 0;
+    float* out = nullptr;
+    Kind kind = Kind::PathTraced;
+    // shared with API threads (guarded by the server mutex)
+    uint32_t status = AR_JOB_PENDING;
+    int32_t error = 0;
+    double t_submit = 0, t_admit = 0, t_done = 0;
+    uint64_t samples = 0;
+    // worker-owned
+    void* films = nullptr;
+    size_t films_bytes = 0;
+    void* scratch = nullptr;  // f32 output (and f32 copies of GDPT films)
+    size_t scratch_bytes = 0;
+    uint32_t slot = kInvalid;
+    uint64_t total_paths = 0;
+    uint64_t bd_next = 0, bd_last_batch = 0;
+    bool bd_issued = false;
+    cudaEvent_t fin = nullptr;
+    cudaStream_t fin_stream = nullptr;
+};
+
+}  // namespace
+
+struct ServerImpl {
+    int device = 0;
+    ar_server_opts opts{};
+    ar_context* ctx_pt = nullptr;
+    ar_context* ctx_bd = nullptr;
+    PathEngine* engine = nullptr;
+    BdptBatcher* bdpt = nullptr;
+    DevicePool pool;
+    std::chrono::steady_clock::time_point t0;
+
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    bool stop = false;
+    uint64_t next_id = 1;
+    std::unordered_map<uint64_t, std::unique_ptr<SJob>> jobs;
+    std::deque<SJob*> incoming;
+
+    // worker state
+    std::deque<SJob*> pending;
+    std::vector<SJob*> active_pt, active_bd, finishing;
+    std::vector<uint32_t> free_slots;
+    uint64_t film_in_use = 0;
+    ar_server_stats stats{};
+    // PT tick throttle and done snapshots
+    static constexpr int kInflight = 4;
+    cudaEvent_t tick_ev[kInflight] = {};
+    uint64_t tick_count = 0;
+    cudaEvent_t snap_ev = nullptr;
+    bool snap_pending = false;
+    // BDPT batches in flight
+    cudaEvent_t bd_ev[2] = {};
+    uint64_t bd_issued_batches = 0, bd_done_batches = 0;
+    std::thread worker;
+
+    double now_ms() const {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+
+    void fail(SJob* j, int code) {
+        std::lock_guard<std::mutex> lk(mu);
+        j->status = AR_JOB_FAILED;
+        j->error = code;
+        j->t_done = now_ms();
+        stats.jobs_failed++;
+        cv_done.notify_all();
+    }
+
+    size_t footprint(const SJob* j) const {
+        const size_t px = size_t(j->w) * j->h * 3;
+        const bool f64 = j->cfg.film_precision == AR_FILM_F64;
+        const int nf = j->cfg.integrator == AR_INTEGRATOR_GDPT ? 3 : 1;
+        return DevicePool::round(px * (f64 ? 8 : 4) * nf) + DevicePool::round(px * 4 * (nf == 3 ? 4 : 1));
+    }
+
+    void admit() {
+        std::vector<std::pair<uint32_t, JobDev>> adds;
+        while (!pending.empty()) {
+            SJob* j = pending.front();
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                if (j->status != AR_JOB_PENDING) {  // cancelled while queued
+                    pending.pop_front();
+                    continue;
+                }
+            }
+            const size_t fp = footprint(j);
+            if (fp > opts.film_budget_bytes) {
+                pending.pop_front();
+                std::lock_guard<std::mutex> lk(mu);
+                j->status = AR_JOB_REJECTED;
+                j->t_done = now_ms();
+                stats.jobs_rejected++;
+                cv_done.notify_all();
+                continue;
+            }
+            if (film_in_use + fp > opts.film_budget_bytes) break;
+            if (j->kind == Kind::PathTraced && free_slots.empty()) break;
+            if (j->kind == Kind::Bidirectional && active_bd.size() >= kMaxBdptJobs) break;
+            pending.pop_front();
+            const bool f64 = j->cfg.film_precision == AR_FILM_F64;
+            const int nf = j->cfg.integrator == AR_INTEGRATOR_GDPT ? 3 : 1;
+            const size_t px = size_t(j->w) * j->h * 3;
+            j->films_bytes = px * (f64 ? 8 : 4) * nf;
+            j->scratch_bytes = px * 4 * (nf == 3 ? 4 : 1);
+            j->films = pool.get(j->films_bytes);
+            j->scratch = pool.get(j->scratch_bytes);
+            film_in_use += fp;
+            stats.film_bytes_in_use = film_in_use;
+            stats.film_bytes_peak = std::max(stats.film_bytes_peak, film_in_use);
+            const CameraDev cam = make_camera(j->cam);
+            if (j->kind == Kind::PathTraced) {
+                AR_CUDA(cudaMemsetAsync(j->films, 0, j->films_bytes, ctx_pt->stream));
+                j->slot = free_slots.back();
+                free_slots.pop_back();
+                JobDev J{};
+                J.sc = j->scene->view;
+                J.cam = cam;
+                J.width = j->w;
+                J.height = j->h;
+                J.spp = j->cfg.spp;
+                J.max_depth = j->cfg.max_depth;
+                J.rr_depth = j->cfg.rr_depth;
+                J.gdpt = nf == 3 ? 1u : 0u;
+                J.film64 = f64 ? 1u : 0u;
+                J.roles = uint32_t(nf);
+                J.seed = j->cfg.seed;
+                J.inv_spp = 1.0f / float(j->cfg.spp);
+                for (int f = 0; f < nf; ++f) J.film[f] = static_cast<char*>(j->films) + f * (px * (f64 ? 8 : 4));
+                J.total_samples = j->samples;
+                J.total_paths = j->samples * uint64_t(nf);
+                j->total_paths = J.total_paths;
+                adds.push_back({j->slot, J});
+                active_pt.push_back(j);
+            } else {
+                AR_CUDA(cudaMemsetAsync(j->films, 0, j->films_bytes, ctx_bd->stream));
+                active_bd.push_back(j);
+            }
+            std::lock_guard<std::mutex> lk(mu);
+            j->status = AR_JOB_RUNNING;
+            j->t_admit = now_ms();
+        }
+        if (!adds.empty()) engine_update(engine, adds, {});
+    }
+
+    // Converts / reconstructs the film and copies it to the caller's buffer.
+    void finish(SJob* j, ar_context* c) {
+        const size_t count = size_t(j->w) * j->h * 3;
+        const bool f64 = j->cfg.film_precision == AR_FILM_F64;
+        float* outd = static_cast<float*>(j->scratch);
+        if (j->cfg.integrator == AR_INTEGRATOR_GDPT) {
+            float* f32 = outd + count;
+            const size_t fb = count * (f64 ? 8 : 4);
+            for (int f = 0; f < 3; ++f)
+                film_to_f32(c, static_cast<char*>(j->films) + f * fb, f64, count, f32 + f * count);
+            poisson_reconstruct(c, j->cfg, j->w, j->h, f32, f32 + count, f32 + 2 * count, outd, nullptr);
+        } else {
+            film_to_f32(c, j->films, f64, count, outd);
+        }
+        AR_CUDA(cudaMemcpyAsync(j->out, outd, count * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+        AR_CUDA(cudaEventCreateWithFlags(&j->fin, cudaEventDisableTiming));
+        AR_CUDA(cudaEventRecord(j->fin, c->stream));
+        j->fin_stream = c->stream;
+        finishing.push_back(j);
+    }
+
+    void step_pt() {
+        if (active_pt.empty()) return;
+        // at most kInflight ticks queued ahead of the GPU
+        cudaEvent_t& ev = tick_ev[tick_count % kInflight];
+        if (tick_count >= kInflight) AR_CUDA(cudaEventSynchronize(ev));
+        engine_tick(engine);
+        AR_CUDA(cudaEventRecord(ev, ctx_pt->stream));
+        tick_count++;
+        stats.pt_ticks++;
+        if (snap_pending && cudaEventQuery(snap_ev) == cudaSuccess) {
+            snap_pending = false;
+            const unsigned long long* done = engine_snapshot_host(engine);
+            std::vector<uint32_t> removes;
+            std::vector<SJob*> still;
+            for (SJob* j : active_pt) {
+                if (done[j->slot] >= j->total_paths) {
+                    removes.push_back(j->slot);
+                    finish(j, ctx_pt);
+                } else {
+                    still.push_back(j);
+                }
+            }
+            active_pt.swap(still);
+            if (!removes.empty()) engine_update(engine, {}, removes);
+        }
+        if (!snap_pending) {
+            engine_snapshot_done(engine);
+            AR_CUDA(cudaEventRecord(snap_ev, ctx_pt->stream));
+            snap_pending = true;
+        }
+    }
+
+    void step_bd() {
+        // reap finished batches
+        while (bd_done_batches < bd_issued_batches &&
+               cudaEventQuery(bd_ev[bd_done_batches % 2]) == cudaSuccess)
+            bd_done_batches++;
+        if (!active_bd.empty()) {
+            std::vector<SJob*> still;
+            for (SJob* j : active_bd) {
+                if (j->bd_issued && j->bd_last_batch <= bd_done_batches) finish(j, ctx_bd);
+                else still.push_back(j);
+            }
+            active_bd.swap(still);
+        }
+        if (bd_issued_batches - bd_done_batches >= 2) return;  // two batches in flight
+        std::vector<BdJob> jobs;
+        std::vector<BdSegment> segs;
+        std::vector<SJob*> members;
+        const uint32_t cap = bdpt_batch_capacity(bdpt);
+        uint32_t used = 0;
+        for (SJob* j : active_bd) {
+            if (j->bd_issued) continue;
+            if (used >= cap) break;
+            const uint64_t rem = j->samples - j->bd_next;
+            const uint32_t take = uint32_t(std::min<uint64_t>(rem, cap - used));
+            const CameraDev cam = make_camera(j->cam);
+            segs.push_back(BdSegment{uint32_t(jobs.size()), used, take, 0, j->bd_next});
+            jobs.push_back(make_bdpt_job(j->scene, cam, j->cfg, j->w, j->h, j->films));
+            members.push_back(j);
+            j->bd_next += take;
+            used += take;
+        }
+        if (segs.empty()) return;
+        bdpt_run_batch(bdpt, jobs, segs);
+        AR_CUDA(cudaEventRecord(bd_ev[bd_issued_batches % 2], ctx_bd->stream));
+        bd_issued_batches++;
+        stats.bdpt_batches++;
+        for (SJob* j : members) {
+            j->bd_last_batch = bd_issued_batches;
+            if (j->bd_next >= j->samples) j->bd_issued = true;
+        }
+    }
+
+    void reap() {
+        std::vector<SJob*> still;
+        for (SJob* j : finishing) {
+            if (cudaEventQuery(j->fin) != cudaSuccess) {
+                still.push_back(j);
+                continue;
+            }
+            cudaEventDestroy(j->fin);
+            j->fin = nullptr;
+            pool.put(j->films, j->films_bytes);
+            pool.put(j->scratch, j->scratch_bytes);
+            j->films = j->scratch = nullptr;
+            film_in_use -= footprint(j);
+            stats.film_bytes_in_use = film_in_use;
+            if (j->slot != kInvalid) free_slots.push_back(j->slot);
+            j->slot = kInvalid;
+            std::lock_guard<std::mutex> lk(mu);
+            j->status = AR_JOB_DONE;
+            j->t_done = now_ms();
+            stats.jobs_done++;
+            stats.path_samples_done += j->samples;
+            cv_done.notify_all();
+        }
+        finishing.swap(still);
+    }
+
+    bool busy() const { return !pending.empty() || !active_pt.empty() || !active_bd.empty() || !finishing.empty(); }
+
+    void run() {
+        AR_CUDA(cudaSetDevice(device));
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                if (!busy() && incoming.empty()) {
+                    if (stop) break;
+                    cv_work.wait_for(lk, std::chrono::milliseconds(2));
+                }
+                while (!incoming.empty()) {
+                    SJob* j = incoming.front();
+                    incoming.pop_front();
+                    if (j->status == AR_JOB_PENDING) pending.push_back(j);
+                }
+            }
+            try {
+                admit();
+                step_pt();
+                step_bd();
+                reap();
+            } catch (const ArError& e) {
+                set_error(e.msg);
+                for (SJob* j : active_pt) fail(j, e.code);
+                for (SJob* j : active_bd) fail(j, e.code);
+                for (SJob* j : finishing) fail(j, e.code);
+                active_pt.clear();
+                active_bd.clear();
+                finishing.clear();
+            }
+            if (!busy()) {
+                // idle: release throttle state so the next burst starts clean
+                std::unique_lock<std::mutex> lk(mu);
+                if (incoming.empty() && stop) break;
+            }
+        }
+    }
+};
+
+}  // namespace ar
+
+struct ar_server {
+    std::unique_ptr<ar::ServerImpl> impl;
+};
+
+using namespace ar;
+
+extern "C" {
+
+int ar_server_create(ar_context* ctx, const ar_server_opts* o, ar_server** out) {
+    return guarded([&] {
+        AR_REQUIRE(ctx && out, AR_ERR_INVALID_ARGUMENT, "null argument");
+        auto s = std::make_unique<ar_server>();
+        s->impl = std::make_unique<ServerImpl>();
+        ServerImpl& S = *s->impl;
+        S.device = ctx->device;
+        if (o) S.opts = *o;
+        if (!S.opts.film_budget_bytes) S.opts.film_budget_bytes = 8ull << 30;
+        if (!S.opts.path_capacity) S.opts.path_capacity = 1u << 21;
+        if (!S.opts.bdpt_batch_samples) S.opts.bdpt_batch_samples = 1u << 18;
+        if (!S.opts.bdpt_max_depth) S.opts.bdpt_max_depth = 10;
+        if (!S.opts.max_active_jobs || S.opts.max_active_jobs > kMaxActiveJobs) S.opts.max_active_jobs = kMaxActiveJobs;
+        S.t0 = std::chrono::steady_clock::now();
+        S.ctx_pt = context_create_internal(ctx->device);
+        S.ctx_bd = context_create_internal(ctx->device);
+        S.engine = engine_create(S.ctx_pt, S.opts.path_capacity);
+        S.bdpt = bdpt_create(S.ctx_bd, S.opts.bdpt_max_depth, S.opts.bdpt_batch_samples);
+        for (uint32_t i = S.opts.max_active_jobs; i-- > 0;) S.free_slots.push_back(i);
+        for (auto& e : S.tick_ev) AR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        for (auto& e : S.bd_ev) AR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        AR_CUDA(cudaEventCreateWithFlags(&S.snap_ev, cudaEventDisableTiming));
+        AR_CUDA(cudaStreamSynchronize(S.ctx_pt->stream));
+        AR_CUDA(cudaStreamSynchronize(S.ctx_bd->stream));
+        S.worker = std::thread([&S] { S.run(); });
+        *out = s.release();
+    });
+}
+
+int ar_server_destroy(ar_server* s) {
+    return guarded([&] {
+        if (!s) return;
+        ServerImpl& S = *s->impl;
+        {
+            std::lock_guard<std::mutex> lk(S.mu);
+            S.stop = true;
+        }
+        S.cv_work.notify_all();
+        if (S.worker.joinable()) S.worker.join();
+        cudaSetDevice(S.device);
+        cudaStreamSynchronize(S.ctx_pt->stream);
+        cudaStreamSynchronize(S.ctx_bd->stream);
+        for (auto& e : S.tick_ev) cudaEventDestroy(e);
+        for (auto& e : S.bd_ev) cudaEventDestroy(e);
+        cudaEventDestroy(S.snap_ev);
+        engine_destroy(S.engine);
+        bdpt_destroy(S.bdpt);
+        context_destroy_internal(S.ctx_pt);
+        context_destroy_internal(S.ctx_bd);
+        delete s;
+    });
+}
+
+int ar_job_submit(ar_server* s, const ar_scene* scene, const ar_camera_desc* camera, const ar_integrator_cfg* cfg,
+                  uint32_t width, uint32_t height, float* out_rgb, uint64_t* job_id) {
+    return guarded([&] {
+        AR_REQUIRE(s && scene && camera && cfg && out_rgb && job_id, AR_ERR_INVALID_ARGUMENT, "null argument");
+        AR_REQUIRE(width > 0 && height > 0 && cfg->spp > 0, AR_ERR_INVALID_ARGUMENT, "empty job");
+        AR_REQUIRE(cfg->integrator <= AR_INTEGRATOR_GDPT, AR_ERR_INVALID_ARGUMENT, "unknown integrator");
+        ServerImpl& S = *s->impl;
+        AR_REQUIRE(scene->device == S.device, AR_ERR_INVALID_ARGUMENT, "scene lives on another device");
+        if (cfg->integrator == AR_INTEGRATOR_BDPT)
+            AR_REQUIRE(cfg->max_depth <= S.opts.bdpt_max_depth, AR_ERR_INVALID_ARGUMENT,
+                       "BDPT max_depth above the server's bdpt_max_depth");
+        else
+            AR_REQUIRE(cfg->max_depth <= 255, AR_ERR_INVALID_ARGUMENT, "max_depth must be <= 255");
+        auto j = std::make_unique<SJob>();
+        j->scene = scene;
+        j->cam = *camera;
+        j->cfg = *cfg;
+        j->w = width;
+        j->h = height;
+        j->out = out_rgb;
+        j->kind = cfg->integrator == AR_INTEGRATOR_BDPT ? Kind::Bidirectional : Kind::PathTraced;
+        j->samples = uint64_t(width) * height * cfg->spp;
+        {
+            std::lock_guard<std::mutex> lk(S.mu);
+            j->id = S.next_id++;
+            j->t_submit = S.now_ms();
+            *job_id = j->id;
+            S.incoming.push_back(j.get());
+            S.stats.jobs_submitted++;
+            S.jobs[j->id] = std::move(j);
+        }
+        S.cv_work.notify_one();
+    });
+}
+
+static void fill_info(const SJob& j, ar_job_info* info) {
+    info->status = j.status;
+    info->error = j.error;
+    info->submit_ms = j.t_submit;
+    info->admit_ms = j.t_admit;
+    info->done_ms = j.t_done;
+    info->path_samples = j.samples;
+}
+
+int ar_job_poll(ar_server* s, uint64_t id, ar_job_info* info) {
+    return guarded([&] {
+        AR_REQUIRE(s && info, AR_ERR_INVALID_ARGUMENT, "null argument");
+        ServerImpl& S = *s->impl;
+        std::lock_guard<std::mutex> lk(S.mu);
+        auto it = S.jobs.find(id);
+        AR_REQUIRE(it != S.jobs.end(), AR_ERR_NOT_FOUND, "unknown job id");
+        fill_info(*it->second, info);
+    });
+}
+
+int ar_job_wait(ar_server* s, uint64_t id, double timeout_ms, ar_job_info* info) {
+    return guarded([&] {
+        AR_REQUIRE(s, AR_ERR_INVALID_ARGUMENT, "null argument");
+        ServerImpl& S = *s->impl;
+        std::unique_lock<std::mutex> lk(S.mu);
+        auto it = S.jobs.find(id);
+        AR_REQUIRE(it != S.jobs.end(), AR_ERR_NOT_FOUND, "unknown job id");
+        SJob* j = it->second.get();
+        const auto deadline = std::chrono::steady_clock::now() + std::chrono::duration<double, std::milli>(timeout_ms);
+        while (j->status == AR_JOB_PENDING || j->status == AR_JOB_RUNNING) {
+            if (S.cv_done.wait_until(lk, deadline) == std::cv_status::timeout &&
+                (j->status == AR_JOB_PENDING || j->status == AR_JOB_RUNNING)) {
+                if (info) fill_info(*j, info);
+                throw ArError{AR_ERR_TIMEOUT, "job still running"};
+            }
+        }
+        if (info) fill_info(*j, info);
+    });
+}
+
+int ar_job_cancel(ar_server* s, uint64_t id) {
+    return guarded([&] {
+        AR_REQUIRE(s, AR_ERR_INVALID_ARGUMENT, "null argument");
+        ServerImpl& S = *s->impl;
+        std::lock_guard<std::mutex> lk(S.mu);
+        auto it = S.jobs.find(id);
+        AR_REQUIRE(it != S.jobs.end(), AR_ERR_NOT_FOUND, "unknown job id");
+        SJob* j = it->second.get();
+        // Only jobs not yet admitted can be withdrawn; the worker skips them.
+        AR_REQUIRE(j->status == AR_JOB_PENDING, AR_ERR_NOT_FOUND, "job already admitted or finished");
+        auto q = std::find(S.incoming.begin(), S.incoming.end(), j);
+        if (q != S.incoming.end()) S.incoming.erase(q);
+        j->status = AR_JOB_CANCELLED;
+        j->t_done = S.now_ms();
+        S.stats.jobs_cancelled++;
+        S.cv_done.notify_all();
+    });
+}
+
+int ar_server_get_stats(ar_server* s, ar_server_stats* out) {
+    return guarded([&] {
+        AR_REQUIRE(s && out, AR_ERR_INVALID_ARGUMENT, "null argument");
+        std::lock_guard<std::mutex> lk(s->impl->mu);
+        *out = s->impl->stats;
+    });
+}
+
+double ar_server_now_ms(ar_server* s) { return s ? s->impl->now_ms() : 0.0; }
+
+}  // extern "C"

@@ -245,12 +245,9 @@ def run_ours(args, rank, local, world):
     for _ in range(max(3, args.warmup)):
         pt.render(scene, cam, W, H, out=out)
     torch.cuda.synchronize()
-    ctx.profile(True)
-    ctx.profile_reset()
     barrier()
     torch.cuda.synchronize()
     step_ms = []
-    launches = 0
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             flush.zero_()
@@ -262,9 +259,17 @@ def run_ours(args, rank, local, world):
             step_ms.append((e0, e1))
         torch.cuda.synchronize()
     st = ctx.render_stats()
-    # per render: generate + (extend, shade, shadow) x depth + counter fold, per chunk
-    launches = args.steps * (st["extend_launches"] * 3 + 2 * (st["extend_launches"] // cfg.max_depth))
+    # per render: `ticks` graph replays of (plan, generate, extend, shade, shadow)
+    launches = args.steps * st["extend_launches"] * 5
     barrier()
+    # Instrumented pass (same workload, same number of renders): the stages are
+    # launched individually with CUDA events on the library stream.
+    ctx.profile(True)
+    ctx.profile_reset()
+    for _ in range(args.steps):
+        flush.zero_()
+        pt.render(scene, cam, W, H, out=out)
+    torch.cuda.synchronize()
     ctx.profile(False)
     prof = ctx.profile_read()
     total_ms = sum(a.elapsed_time(b) for a, b in step_ms)

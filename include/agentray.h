@@ -253,6 +253,63 @@ int ar_poisson_reconstruct(ar_context* ctx, const ar_integrator_cfg* cfg, uint32
                            const float* primal, const float* grad_x, const float* grad_y, float* out,
                            uint32_t on_device, double* rel_residual);
 
+/* ---- serving (no counterpart in the reference: it renders one job per call) ----
+ * A server owns a worker thread that continuously batches every admitted job
+ * into shared wavefront kernels: PT and GDPT paths stream through one path pool
+ * refilled every tick; BDPT jobs share sample batches.  Jobs are admitted in
+ * arrival order while their films fit the HBM budget; a job whose films alone
+ * exceed the budget is REJECTED.  Results are written to the caller's host
+ * buffer (W*H*3 f32, like ar_render) before the job reports DONE. */
+typedef struct ar_server ar_server;
+
+enum ar_job_status {
+    AR_JOB_PENDING = 0,
+    AR_JOB_RUNNING = 1,
+    AR_JOB_DONE = 2,
+    AR_JOB_REJECTED = 3,
+    AR_JOB_CANCELLED = 4,
+    AR_JOB_FAILED = 5
+};
+
+typedef struct ar_server_opts {
+    uint64_t film_budget_bytes;      /* HBM for job films (0: 8 GiB) */
+    uint32_t path_capacity;          /* path slots of the streaming engine (0: 2^21) */
+    uint32_t bdpt_batch_samples;     /* samples per BDPT batch (0: 2^18) */
+    uint32_t bdpt_max_depth;         /* largest BDPT max_depth accepted (0: 10) */
+    uint32_t max_active_jobs;        /* 0: 1024 */
+} ar_server_opts;
+
+typedef struct ar_job_info {
+    uint32_t status;                 /* ar_job_status */
+    int32_t error;                   /* ar_status of a FAILED job */
+    double submit_ms, admit_ms, done_ms;  /* server clock */
+    uint64_t path_samples;
+} ar_job_info;
+
+typedef struct ar_server_stats {
+    uint64_t jobs_submitted, jobs_done, jobs_rejected, jobs_cancelled, jobs_failed;
+    uint64_t path_samples_done;
+    uint64_t pt_ticks, bdpt_batches;
+    uint64_t film_bytes_in_use, film_bytes_peak;
+} ar_server_stats;
+
+int ar_server_create(ar_context* ctx, const ar_server_opts* opts, ar_server** out);
+/* Waits for admitted jobs to finish, then stops the worker. */
+int ar_server_destroy(ar_server* server);
+/* Non-blocking: queues the job and returns its id.  `scene` must stay alive
+ * until the job finishes; `out_rgb` (host, W*H*3 floats) receives the image. */
+int ar_job_submit(ar_server* server, const ar_scene* scene, const ar_camera_desc* camera,
+                  const ar_integrator_cfg* cfg, uint32_t width, uint32_t height, float* out_rgb,
+                  uint64_t* job_id);
+int ar_job_poll(ar_server* server, uint64_t job_id, ar_job_info* info);
+/* Blocks until the job leaves PENDING/RUNNING or timeout_ms passes
+ * (AR_ERR_TIMEOUT). */
+int ar_job_wait(ar_server* server, uint64_t job_id, double timeout_ms, ar_job_info* info);
+/* Cancels a job that has not been admitted yet (AR_ERR_NOT_FOUND otherwise). */
+int ar_job_cancel(ar_server* server, uint64_t job_id);
+int ar_server_get_stats(ar_server* server, ar_server_stats* out);
+double ar_server_now_ms(ar_server* server);
+
 /* ---- instrumentation (no counterpart in the reference) ---- */
 
 /* Work counters of the last ar_render on this context. */

@@ -1,0 +1,98 @@
+"""GPU serving tests: continuous batching must not change any job's result.
+
+Each job keys its sample stream by (seed, pixel, sample), so a job rendered
+alone (ar_render) and the same job rendered by the server while other jobs of
+other scenes/resolutions/integrators share its kernels must agree; with f64
+films the only difference is the order of floating-point atomics
+(tolerance: 1e-5 relative)."""
+import numpy as np
+import pytest
+
+import agentray
+import agentray.scenes as S
+from agentray import _abi as A
+
+pytestmark = pytest.mark.gpu
+
+
+def _pt(spp, depth=8, seed=0, f64=True):
+    return agentray.PathTracer(agentray.PathTracerConfig(spp=spp, max_depth=depth, rr_depth=3, seed=seed,
+                                                         film_precision=A.FILM_F64 if f64 else A.FILM_F32))
+
+
+def _bdpt(spp, depth=6, seed=0, f64=True):
+    return agentray.BidirectionalPathTracer(agentray.BdptConfig(spp=spp, max_depth=depth, rr_depth=3, seed=seed,
+                                                                film_precision=A.FILM_F64 if f64 else A.FILM_F32))
+
+
+def _gdpt(spp, seed=0):
+    return agentray.GradientDomainPathTracer(agentray.GdptConfig(spp=spp, max_depth=6, seed=seed,
+                                                                 film_precision=A.FILM_F64))
+
+
+def test_alone_equals_mixed(ctx):
+    cb, cb_cam = S.cornell_box(1)
+    s0, s0_cam = S.served_scene(0)
+    scenes = {"cornell": agentray.Scene(ctx, cb), "served0": agentray.Scene(ctx, s0)}
+    cams = {"cornell": cb_cam, "served0": s0_cam}
+    jobs = [("cornell", _pt(16, seed=1), 64, 64), ("served0", _pt(4, seed=2), 96, 80),
+            ("cornell", _bdpt(8, seed=3), 48, 48), ("served0", _bdpt(4, seed=4), 64, 64),
+            ("cornell", _gdpt(8, seed=5), 64, 48)]
+    alone = [integ.render(scenes[s], cams[s], w, h).rgb.copy() for s, integ, w, h in jobs]
+    srv = agentray.Server(ctx, path_capacity=1 << 18, bdpt_batch_samples=1 << 14)
+    ids = []
+    # interleave the checked jobs with filler jobs of other sizes
+    for k, (s, integ, w, h) in enumerate(jobs):
+        ids.append(srv.submit(scenes[s], cams[s], integ, w, h))
+        srv.submit(scenes["served0"], s0_cam, _pt(4, seed=100 + k, f64=False), 128, 128)
+        srv.submit(scenes["cornell"], cb_cam, _bdpt(2, seed=200 + k, f64=False), 32, 32)
+    for jid in ids:
+        assert srv.wait(jid)["status"] == "done"
+    for jid, ref in zip(ids, alone):
+        out = srv.result(jid)
+        np.testing.assert_allclose(out, ref, rtol=1e-5, atol=1e-6)
+    st = srv.stats()
+    srv.close()
+    assert st["jobs_done"] >= len(jobs)
+    assert st["pt_ticks"] > 0 and st["bdpt_batches"] > 0
+
+
+def test_rejection_and_cancellation(ctx):
+    cb, cam = S.cornell_box(1)
+    scene = agentray.Scene(ctx, cb)
+    # budget fits one 64x64 f32 job at a time, not a 1024x1024 one
+    srv = agentray.Server(ctx, film_budget_bytes=4 << 20, path_capacity=1 << 16)
+    big = srv.submit(scene, cam, _pt(1, f64=False), 1024, 1024)
+    queued = [srv.submit(scene, cam, _pt(64, f64=False), 64, 64) for _ in range(6)]
+    victim = queued[-1]
+    try:
+        srv.cancel(victim)
+        cancelled = True
+    except agentray.AgentRayError:
+        cancelled = False  # the worker admitted it first
+    assert srv.wait(big)["status"] == "rejected"
+    for jid in queued[:-1]:
+        info = srv.wait(jid)
+        assert info["status"] == "done"
+        assert info["admit_ms"] >= info["submit_ms"] and info["done_ms"] >= info["admit_ms"]
+    if cancelled:
+        assert srv.poll(victim)["status"] == "cancelled"
+    st = srv.stats()
+    srv.close()
+    assert st["jobs_rejected"] == 1
+    assert st["film_bytes_peak"] <= 4 << 20
+    assert st["film_bytes_in_use"] == 0
+
+
+def test_server_results_match_plain_path_f32(ctx):
+    # Default f32 films: same images up to atomic ordering.
+    s1, cam = S.served_scene(1)
+    scene = agentray.Scene(ctx, s1)
+    integ = _pt(8, seed=9, f64=False)
+    ref = integ.render(scene, cam, 128, 128).rgb.copy()
+    srv = agentray.Server(ctx)
+    jid = srv.submit(scene, cam, integ, 128, 128)
+    assert srv.wait(jid)["status"] == "done"
+    out = srv.result(jid)
+    srv.close()
+    np.testing.assert_allclose(out, ref, rtol=1e-4, atol=1e-5)

@@ -259,16 +259,26 @@ class Server:
         self.outputs = {}
         self._keep = {}
 
-    def submit(self, scene: Scene, camera: Camera, integrator, width, height):
-        out = np.empty(width * height * 3, np.float32)
+    def submit(self, scene: Scene, camera: Camera, integrator, width, height, out=None):
+        """Queues a job.  `out` may be a host numpy buffer (default: a new one)
+        or a CUDA float32 tensor of W*H*3 elements to keep the image on the GPU."""
+        on_device = out is not None and not isinstance(out, np.ndarray)
+        if out is None:
+            out = np.empty(width * height * 3, np.float32)
+        ptr = out.data_ptr() if on_device else out.ctypes.data
         cam = camera.desc()
         cfg = integrator.cfg()
         jid = C.c_uint64()
-        check(lib().ar_job_submit(self.handle, scene.handle, C.byref(cam), C.byref(cfg), width, height,
-                                  out.ctypes.data, C.byref(jid)))
-        self.outputs[jid.value] = out.reshape(height, width, 3)
+        check(lib().ar_job_submit(self.handle, scene.handle, C.byref(cam), C.byref(cfg), width, height, ptr,
+                                  1 if on_device else 0, C.byref(jid)))
+        self.outputs[jid.value] = out if on_device else out.reshape(height, width, 3)
         self._keep[jid.value] = scene
         return jid.value
+
+    def forget(self, job_id):
+        """Drops the Python-side references of a finished job."""
+        self.outputs.pop(job_id, None)
+        self._keep.pop(job_id, None)
 
     @staticmethod
     def _info(i):
@@ -298,6 +308,11 @@ class Server:
 
     def now_ms(self):
         return lib().ar_server_now_ms(self.handle)
+
+    def debug_dump(self):
+        buf = C.create_string_buffer(1 << 16)
+        check(lib().ar_server_debug_dump(self.handle, buf, 1 << 16))
+        return buf.value.decode()
 
     def close(self):
         if self.handle:

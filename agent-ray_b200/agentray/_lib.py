@@ -34,12 +34,13 @@ SIGNATURES = {
     "ar_server_create": (C.c_int, [C.c_void_p, C.POINTER(A.ServerOpts), C.POINTER(C.c_void_p)]),
     "ar_server_destroy": (C.c_int, [C.c_void_p]),
     "ar_job_submit": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(A.CameraDesc), C.POINTER(A.IntegratorCfg),
-                                C.c_uint32, C.c_uint32, C.c_void_p, C.POINTER(C.c_uint64)]),
+                                C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint64)]),
     "ar_job_poll": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(A.JobInfo)]),
     "ar_job_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.c_double, C.POINTER(A.JobInfo)]),
     "ar_job_cancel": (C.c_int, [C.c_void_p, C.c_uint64]),
     "ar_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(A.ServerStats)]),
     "ar_server_now_ms": (C.c_double, [C.c_void_p]),
+    "ar_server_debug_dump": (C.c_int, [C.c_void_p, C.c_char_p, C.c_uint32]),
     "ar_get_render_stats": (C.c_int, [C.c_void_p, C.POINTER(A.RenderStats)]),
     "ar_profile_enable": (C.c_int, [C.c_void_p, C.c_int]),
     "ar_profile_reset": (C.c_int, [C.c_void_p]),

@@ -234,12 +234,18 @@ def served_scene(k, seed=5):
     n_boxes = min(300, max(20, remaining // 200))
     remaining -= 12 * n_boxes
     sphere_meshes = {}
+    eye = np.array([5.0, 2.5, 9.6])
+
+    def clear_of_eye(p, radius):
+        return np.linalg.norm(np.asarray(p) - eye) > radius + 0.6
     while remaining >= 20 * 4 ** 2:
         lvl = max(l for l in range(2, 9) if 20 * 4 ** l <= remaining)
         if lvl not in sphere_meshes:
             sphere_meshes[lvl] = sc.add_mesh(icosphere(lvl))
         r = float(rng.uniform(0.4, 1.2))
         ctr = (rng.uniform(1.0, W - 1.0), r, rng.uniform(1.0, D - 1.0))
+        while not clear_of_eye(ctr, r):
+            ctr = (rng.uniform(1.0, W - 1.0), r, rng.uniform(1.0, D - 1.0))
         xf, inv = trs(ctr, None, (r, r, r))
         sc.add_object(Object(sphere_meshes[lvl], [sc.add_material(random_material(rng))], xf, inv))
         remaining -= 20 * 4 ** lvl
@@ -248,6 +254,8 @@ def served_scene(k, seed=5):
     for _ in range(n_boxes):
         s = rng.uniform(0.1, 0.5, 3)
         t = (rng.uniform(0.3, W - 0.3), rng.uniform(0.2, H - 0.6), rng.uniform(0.3, D - 0.3))
+        while not clear_of_eye(t, 0.45):
+            t = (rng.uniform(0.3, W - 0.3), rng.uniform(0.2, H - 0.6), rng.uniform(0.3, D - 0.3))
         xf, inv = trs(t, random_rotation(rng), s)
         sc.add_object(Object(cube, [sc.add_material(random_material(rng))], xf, inv))
     add_quad_light(sc, (2.5, 4.99, 4.5), (1.0, 0.0, 0.0), (0.0, 0.0, 1.0), (12.0, 12.0, 12.0))

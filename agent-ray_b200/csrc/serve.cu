@@ -72,6 +72,7 @@ struct SJob {
     ar_integrator_cfg cfg{};
     uint32_t w = 0, h = 0;
     float* out = nullptr;
+    bool out_on_device = false;
     Kind kind = Kind::PathTraced;
     // shared with API threads (guarded by the server mutex)
     uint32_t status = AR_JOB_PENDING;
@@ -86,6 +87,8 @@ struct SJob {
     uint32_t slot = kInvalid;
     uint64_t total_paths = 0;
     uint64_t bd_next = 0, bd_last_batch = 0;
+    uint64_t min_snap = 0;  // first done-counter snapshot issued after admission
+    uint64_t last_done = 0; // done paths seen in the last snapshot (diagnostics)
     bool bd_issued = false;
     cudaEvent_t fin = nullptr;
     cudaStream_t fin_stream = nullptr;
@@ -122,6 +125,7 @@ struct ServerImpl {
     uint64_t tick_count = 0;
     cudaEvent_t snap_ev = nullptr;
     bool snap_pending = false;
+    uint64_t snap_issued = 0;   // id of the last snapshot issued (1-based)
     // BDPT batches in flight
     cudaEvent_t bd_ev[2] = {};
     uint64_t bd_issued_batches = 0, bd_done_batches = 0;
@@ -185,6 +189,7 @@ struct ServerImpl {
             const CameraDev cam = make_camera(j->cam);
             if (j->kind == Kind::PathTraced) {
                 AR_CUDA(cudaMemsetAsync(j->films, 0, j->films_bytes, ctx_pt->stream));
+                j->min_snap = snap_issued + 1;  // an older snapshot predates this job's table entry
                 j->slot = free_slots.back();
                 free_slots.pop_back();
                 JobDev J{};
@@ -231,7 +236,8 @@ struct ServerImpl {
         } else {
             film_to_f32(c, j->films, f64, count, outd);
         }
-        AR_CUDA(cudaMemcpyAsync(j->out, outd, count * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+        AR_CUDA(cudaMemcpyAsync(j->out, outd, count * sizeof(float),
+                                j->out_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c->stream));
         AR_CUDA(cudaEventCreateWithFlags(&j->fin, cudaEventDisableTiming));
         AR_CUDA(cudaEventRecord(j->fin, c->stream));
         j->fin_stream = c->stream;
@@ -253,7 +259,8 @@ struct ServerImpl {
             std::vector<uint32_t> removes;
             std::vector<SJob*> still;
             for (SJob* j : active_pt) {
-                if (done[j->slot] >= j->total_paths) {
+                j->last_done = done[j->slot];
+                if (snap_issued >= j->min_snap && done[j->slot] >= j->total_paths) {
                     removes.push_back(j->slot);
                     finish(j, ctx_pt);
                 } else {
@@ -267,6 +274,7 @@ struct ServerImpl {
             engine_snapshot_done(engine);
             AR_CUDA(cudaEventRecord(snap_ev, ctx_pt->stream));
             snap_pending = true;
+            snap_issued++;
         }
     }
 
@@ -340,6 +348,36 @@ struct ServerImpl {
 
     bool busy() const { return !pending.empty() || !active_pt.empty() || !active_bd.empty() || !finishing.empty(); }
 
+    // Diagnostics: the worker formats its state when asked (its queues are
+    // not shared with API threads).
+    bool debug_requested = false;
+    std::string debug_text;
+    void maybe_dump() {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            if (!debug_requested) return;
+        }
+        std::string s = "ticks=" + std::to_string(tick_count) + " snap_issued=" + std::to_string(snap_issued) +
+                        " snap_pending=" + std::to_string(snap_pending) + " bd_issued=" +
+                        std::to_string(bd_issued_batches) + " bd_done=" + std::to_string(bd_done_batches) +
+                        " film_in_use=" + std::to_string(film_in_use) + " pending=" + std::to_string(pending.size()) +
+                        "\n";
+        for (SJob* j : pending) s += "  pending job " + std::to_string(j->id) + "\n";
+        for (SJob* j : active_pt)
+            s += "  pt job " + std::to_string(j->id) + " slot=" + std::to_string(j->slot) + " done=" +
+                 std::to_string(j->last_done) + "/" + std::to_string(j->total_paths) +
+                 " min_snap=" + std::to_string(j->min_snap) + "\n";
+        for (SJob* j : active_bd)
+            s += "  bdpt job " + std::to_string(j->id) + " next=" + std::to_string(j->bd_next) + "/" +
+                 std::to_string(j->samples) + " issued=" + std::to_string(j->bd_issued) +
+                 " last_batch=" + std::to_string(j->bd_last_batch) + "\n";
+        for (SJob* j : finishing) s += "  finishing job " + std::to_string(j->id) + "\n";
+        std::lock_guard<std::mutex> lk(mu);
+        debug_text = s;
+        debug_requested = false;
+        cv_done.notify_all();
+    }
+
     void run() {
         AR_CUDA(cudaSetDevice(device));
         for (;;) {
@@ -360,6 +398,7 @@ struct ServerImpl {
                 step_pt();
                 step_bd();
                 reap();
+                maybe_dump();
             } catch (const ArError& e) {
                 set_error(e.msg);
                 for (SJob* j : active_pt) fail(j, e.code);
@@ -442,7 +481,7 @@ int ar_server_destroy(ar_server* s) {
 }
 
 int ar_job_submit(ar_server* s, const ar_scene* scene, const ar_camera_desc* camera, const ar_integrator_cfg* cfg,
-                  uint32_t width, uint32_t height, float* out_rgb, uint64_t* job_id) {
+                  uint32_t width, uint32_t height, float* out_rgb, uint32_t out_on_device, uint64_t* job_id) {
     return guarded([&] {
         AR_REQUIRE(s && scene && camera && cfg && out_rgb && job_id, AR_ERR_INVALID_ARGUMENT, "null argument");
         AR_REQUIRE(width > 0 && height > 0 && cfg->spp > 0, AR_ERR_INVALID_ARGUMENT, "empty job");
@@ -461,6 +500,7 @@ int ar_job_submit(ar_server* s, const ar_scene* scene, const ar_camera_desc* cam
         j->w = width;
         j->h = height;
         j->out = out_rgb;
+        j->out_on_device = out_on_device != 0;
         j->kind = cfg->integrator == AR_INTEGRATOR_BDPT ? Kind::Bidirectional : Kind::PathTraced;
         j->samples = uint64_t(width) * height * cfg->spp;
         {
@@ -544,5 +584,23 @@ int ar_server_get_stats(ar_server* s, ar_server_stats* out) {
 }
 
 double ar_server_now_ms(ar_server* s) { return s ? s->impl->now_ms() : 0.0; }
+
+int ar_server_debug_dump(ar_server* s, char* buf, uint32_t capacity) {
+    return guarded([&] {
+        AR_REQUIRE(s && buf && capacity > 0, AR_ERR_INVALID_ARGUMENT, "null argument");
+        ServerImpl& S = *s->impl;
+        std::unique_lock<std::mutex> lk(S.mu);
+        S.debug_requested = true;
+        S.cv_work.notify_all();
+        const auto deadline = std::chrono::steady_clock::now() + std::chrono::seconds(5);
+        while (S.debug_requested)
+            if (S.cv_done.wait_until(lk, deadline) == std::cv_status::timeout) break;
+        std::string t = S.debug_requested ? std::string("worker did not answer within 5 s\n") : S.debug_text;
+        S.debug_requested = false;
+        const size_t n = std::min<size_t>(t.size(), capacity - 1);
+        std::memcpy(buf, t.data(), n);
+        buf[n] = 0;
+    });
+}
 
 }  // extern "C"

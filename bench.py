@@ -1,25 +1,35 @@
 """Benchmark driver: one JSON line on rank 0.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload served|pt_cornell|bvh] [--jobs J]
 
-Workloads (seeded synthetic scenes with the stated shapes; no dataset exists):
-  pt_cornell  (default) unidirectional PT, procedural Cornell box: 5 walls + 2
-              rotated boxes = 34 triangles, 0.25 x 0.25 quad light of radiance
-              15, albedos U[0.2,0.8], 256x256, 16 spp, max depth 8, RR from
-              depth 3, f32 film.  One step = one full render (1,048,576 path
-              samples).  Metric: Mpath-samples/s.
-  bvh         BVH micro-benchmark: 1M triangles, 16M closest-hit rays
-              (secondary line; metric Mrays/s).
+Workloads (seeded synthetic inputs with the stated shapes; no dataset exists):
+  served      (default) the served batched-rendering stream: Poisson arrivals of
+              2000 jobs, scenes drawn from 8 seeded procedural scenes of
+              10k-1M triangles, resolution from {128,256,512,1024}^2, spp from
+              {4,16,64}, PT or BDPT 70/30 (PT: depth 8, RR from 3; BDPT: depth
+              8, RR from 3, power-heuristic MIS).  Metric: Mpath-samples/s.
+              A step is one window of J/(W+K) consecutive jobs submitted to the
+              render server together (continuous batching under a backlog);
+              `value` is the throughput of the K timed windows with images kept
+              on the GPU, `e2e` the same windows' jobs with images returned to
+              pinned host buffers.  `served` adds p50/p99 latency of a Poisson
+              arrival run at 80% of the measured capacity, and `plain` the
+              one-job-at-a-time GPU path (ar_render per job) on the first timed
+              window's jobs.
+  pt_cornell  PT Cornell box (34 tris + quad light, 256x256, 16 spp, depth 8);
+              one step = one full render.
+  bvh         BVH micro-benchmark: 1M triangles, 16M closest-hit rays (Mrays/s).
 
-Timing: W warm-up steps, then K steps, each bracketed by CUDA events on the
-stream the library launches on (the context is bound to torch's current
-stream); L2 is flushed (256 MiB write) before every timed step, outside its
-events.  Multi-GPU: one process per GPU; each rank renders its own job
-(seed = rank; weak scaling, no data-path collective); the time is the max over
-ranks.  `e2e` times the public C-ABI path with host buffers: scene upload from
-host arrays (Scene::new: BVH build + copies) + render + device->host readback.
-`--impl reference` times the reference algorithm on the host cores (the C++
-restatement of agent-ray's CPU integrator, the reference's own sampler).
+Timing: CUDA events on the stream the library launches on (pt_cornell, bvh)
+or, for the server (which runs on its own internal streams), events recorded
+on an idle stream around the window (submission -> last result), i.e. device
+timestamps of the window's wall span.  L2 is flushed (256 MiB write) before
+every timed step outside its events.  Multi-GPU: one process per GPU, each
+rank serves its own seeded stream (weak scaling, no data-path collective);
+time is the max over ranks.  `--impl reference` times the reference algorithm
+(the C++ restatement of agent-ray's CPU integrators with the reference's
+xoshiro sampler) on all host cores on a bounded sample of the same workload.
 """
 import argparse
 import json
@@ -27,6 +37,7 @@ import os
 import statistics
 import subprocess
 import sys
+import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -36,6 +47,8 @@ import numpy as np  # noqa: E402
 
 METRIC = "Mpath-samples/s at equal relMSE, batched vs plain GPU; served p50/p99 latency"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+SERVED_DESC = ("served: Poisson stream of 2000 jobs over 8 procedural scenes (10k-1M tris), res {128..1024}^2, "
+               "spp {4,16,64}, PT/BDPT 70/30, depth 8")
 
 
 def load_peaks():
@@ -84,7 +97,7 @@ class ClockSampler:
     def summary(self):
         if not self.proc or not os.path.exists(self.path):
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm, mx, reasons = [], None, set()
+        sm, mx, reasons, power = [], None, set(), []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in open(self.path):
             parts = [x.strip() for x in line.split(",")]
@@ -93,13 +106,14 @@ class ClockSampler:
             try:
                 sm.append(float(parts[1]))
                 mx = float(parts[2])
+                power.append(float(parts[3]))
             except ValueError:
                 continue
             for n, v in zip(names, parts[5:9]):
                 if v.lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "power_w_median": statistics.median(power) if power else None}
 
 
 def profile_traffic(name):
@@ -113,20 +127,11 @@ def profile_traffic(name):
     return None
 
 
-def reference_traversal_counts(scene_data, cam, w, h, n=65536, seed=7):
-    """Mean AABB tests and triangle tests per ray of the reference binary SAH
-    traversal (oracle counters) on this workload's primary rays and on rays
-    with origins/directions uniform inside the scene bounds (bounce proxy)."""
-    import oracle as O
-    osc = O.OracleScene(scene_data)
-    rng = np.random.default_rng(seed)
-    # primary rays through random pixels
-    from agentray.scene_data import Camera  # noqa: F401
+def camera_rays(cam, n, rng):
     lf = np.array(cam.lookfrom, np.float64)
     la = np.array(cam.lookat, np.float64)
     up = np.array(cam.vup, np.float64)
-    th = np.radians(cam.vfov_deg)
-    vh = 2 * np.tan(th / 2)
+    vh = 2 * np.tan(np.radians(cam.vfov_deg) / 2)
     vw = cam.aspect * vh
     wv = (lf - la) / np.linalg.norm(lf - la)
     u = np.cross(up, wv)
@@ -134,10 +139,20 @@ def reference_traversal_counts(scene_data, cam, w, h, n=65536, seed=7):
     v = np.cross(wv, u)
     ll = lf - vw * u / 2 - vh * v / 2 - wv
     su, sv = rng.uniform(size=(n, 1)), rng.uniform(size=(n, 1))
-    d = ll + su * vw * u + sv * vh * v - lf
+    return np.broadcast_to(lf, (n, 3)), ll + su * vw * u + sv * vh * v - lf
+
+
+def reference_traversal_counts(scene_data, cam, n=32768, seed=7):
+    """Mean AABB tests and triangle tests per ray of the reference binary SAH
+    traversal (oracle counters) on primary rays and on rays uniform inside the
+    scene bounds (a proxy for bounce rays)."""
+    import oracle as O
+    osc = O.OracleScene(scene_data)
+    rng = np.random.default_rng(seed)
+    o, d = camera_rays(cam, n, rng)
     ot = np.zeros((2 * n, 4), np.float32)
     dt = np.zeros((2 * n, 4), np.float32)
-    ot[:n, :3] = lf
+    ot[:n, :3] = o
     ot[:n, 3] = 1e-3
     dt[:n, :3] = d
     dt[:, 3] = np.inf
@@ -148,97 +163,262 @@ def reference_traversal_counts(scene_data, cam, w, h, n=65536, seed=7):
     dd = rng.normal(size=(n, 3))
     dt[n:, :3] = dd / np.linalg.norm(dd, axis=1, keepdims=True)
     r = osc.trace_closest(ot, dt, stats=True)
+    osc.close()
     return r["stats"]["nodes"] / (2 * n), r["stats"]["tris"] / (2 * n)
 
 
-def run_reference(args, rank, world):
-    """--impl reference: the reference CPU algorithm (oracle restatement,
-    xoshiro256++ per-pixel streams like IndependentSampler) on all host cores."""
-    if rank != 0:
-        return
-    import oracle as O
-    import agentray.scenes as S
+def make_integrator(agentray, job, seed):
+    if job["integrator"] == "bdpt":
+        return agentray.BidirectionalPathTracer(agentray.BdptConfig(spp=job["spp"], max_depth=8, rr_depth=3,
+                                                                    seed=seed))
+    return agentray.PathTracer(agentray.PathTracerConfig(spp=job["spp"], max_depth=8, rr_depth=3, seed=seed))
+
+
+def job_cfg(job, seed):
     from agentray import _abi as A
     from agentray.scene_data import integrator_cfg
-    cores = os.cpu_count() or 1
-    sc, cam = S.cornell_box(1)
-    osc = O.OracleScene(sc)
-    cfg = integrator_cfg(A.INTEGRATOR_PT, spp=16, max_depth=8, rr_depth=3)
-    w = h = 256
-    for _ in range(args.warmup):
-        osc.render(cam, cfg, w, h, sampler=O.SAMPLER_XOSHIRO, threads=cores)
-    times = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        osc.render(cam, cfg, w, h, sampler=O.SAMPLER_XOSHIRO, threads=cores)
-        times.append(time.perf_counter() - t0)
-    samples = w * h * cfg.spp
-    value = samples * args.steps / sum(times) / 1e6
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mpath-samples/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded procedural scene)",
-            "config": {"workload": "pt_cornell: PT Cornell box 34 tris + quad light, 256x256, 16 spp, depth 8, RR 3",
-                       "width": w, "height": h, "spp": 16},
-            "cpu_baseline": {"value": value, "unit": "Mpath-samples/s", "cores": cores, "kind": "port",
-                             "sample": "full workload per step (256x256x16 spp)"},
-            "e2e": {"value": value, "unit": "Mpath-samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
+    kind = A.INTEGRATOR_BDPT if job["integrator"] == "bdpt" else A.INTEGRATOR_PT
+    return integrator_cfg(kind, spp=job["spp"], max_depth=8, rr_depth=3, seed=seed)
 
 
-def cpu_baseline_pt(sc, cam, cfg):
-    import oracle as O
-    cores = os.cpu_count() or 1
-    osc = O.OracleScene(sc)
-    w = h = 256
-    osc.render(cam, cfg, 32, 32, sampler=O.SAMPLER_XOSHIRO, threads=cores)
-    t0 = time.perf_counter()
-    reps = 0
-    while True:
-        osc.render(cam, cfg, w, h, sampler=O.SAMPLER_XOSHIRO, threads=cores)
-        reps += 1
-        if time.perf_counter() - t0 > 2.0 or reps >= 10:
+# ----------------------------------------------------------------- served ----
+def wait_or_dump(srv, job_id, timeout_ms=180_000.0):
+    """Waits for a job; on timeout prints the server's queue state and raises."""
+    try:
+        return srv.wait(job_id, timeout_ms)
+    except Exception:
+        print("job", job_id, srv.poll(job_id), "\nserver state:\n" + srv.debug_dump(), "\nstats:", srv.stats(),
+              file=sys.stderr, flush=True)
+        raise
+
+
+def run_served(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind):
+    import agentray
+    import agentray.scenes as S
+
+    n_jobs = args.jobs
+    stream = S.served_stream(n_jobs, seed=5 + 1000 * rank)
+    built = [S.served_scene(k) for k in range(8)]
+    scenes = [agentray.Scene(ctx, sd) for sd, _ in built]
+    cams = [cam for _, cam in built]
+    srv = agentray.Server(ctx, film_budget_bytes=24 << 30, path_capacity=1 << 21, bdpt_batch_samples=1 << 19,
+                          bdpt_max_depth=8)
+    W, K = max(3, args.warmup), args.steps
+    n_burst = int(n_jobs * 0.6)
+    per = max(1, n_burst // (W + K))
+    windows = [stream[i * per:(i + 1) * per] for i in range(W + K)]
+    served_jobs = stream[(W + K) * per:]
+    side = torch.cuda.Stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    dev_out = {128: [], 256: [], 512: [], 1024: []}
+
+    def device_buffer(res, i):
+        pool = dev_out[res]
+        while len(pool) <= i:
+            pool.append(torch.empty(res * res * 3, dtype=torch.float32, device="cuda"))
+        return pool[i]
+
+    def run_window(jobs, host_out, base_seed):
+        counters = {}
+        ids = []
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(side)
+        for i, job in enumerate(jobs):
+            r = job["res"]
+            k = counters.get(r, 0)
+            counters[r] = k + 1
+            out = None if host_out else device_buffer(r, k)
+            ids.append(srv.submit(scenes[job["scene"]], cams[job["scene"]], make_integrator(agentray, job,
+                                                                                           base_seed + i), r, r,
+                                  out=out))
+        infos = [wait_or_dump(srv, j) for j in ids]
+        e1.record(side)
+        torch.cuda.synchronize()
+        for j in ids:
+            srv.forget(j)
+        assert all(i["status"] == "done" for i in infos), [i["status"] for i in infos]
+        samples = sum(j["res"] ** 2 * j["spp"] for j in jobs)
+        return e0.elapsed_time(e1), samples, infos
+
+    # warm-up windows (also calibrate capacity)
+    for w in range(W):
+        run_window(windows[w], False, 10_000 * w)
+    barrier()
+    ms_list, samples_total = [], 0
+    with ClockSampler(local) as clk:
+        for k in range(K):
+            ms, smp, _ = run_window(windows[W + k], False, 10_000 * (W + k))
+            ms_list.append(ms)
+            samples_total += smp
+    total_ms = sum(ms_list)
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    value = world * samples_total / (float(t.item()) / 1e3) / 1e6
+    capacity_sps = samples_total / (total_ms / 1e3)
+
+    # e2e: the first two timed windows again with images returned to host
+    e2e_ms, e2e_samples, d2h = 0.0, 0, 0
+    for k in range(min(2, K)):
+        ms, smp, _ = run_window(windows[W + k], True, 10_000 * (W + k))
+        e2e_ms += ms
+        e2e_samples += smp
+        d2h += sum(j["res"] ** 2 * 3 * 4 for j in windows[W + k])
+    e2e_value = e2e_samples / (e2e_ms / 1e3) / 1e6
+
+    # served: Poisson arrivals at 80% of the measured capacity
+    mean_samples = statistics.mean(j["res"] ** 2 * j["spp"] for j in stream)
+    rate = 0.8 * capacity_sps / mean_samples
+    arrivals = np.cumsum(np.random.default_rng(77 + rank).exponential(1.0 / rate, len(served_jobs)))
+    ids = []
+    t_start = time.perf_counter()
+    counters = {}
+    for i, job in enumerate(served_jobs):
+        delay = arrivals[i] - (time.perf_counter() - t_start)
+        if delay > 0:
+            time.sleep(delay)
+        ids.append(srv.submit(scenes[job["scene"]], cams[job["scene"]], make_integrator(agentray, job, 50_000 + i),
+                              job["res"], job["res"]))
+    infos = [wait_or_dump(srv, j) for j in ids]
+    served_span = time.perf_counter() - t_start
+    lat = np.array([i["done_ms"] - i["submit_ms"] for i in infos])
+    served = {"jobs": len(served_jobs), "arrival_rate_jobs_per_s": rate, "load": 0.8,
+              "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
+              "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
+              "mean_ms": float(lat.mean()) if len(lat) else None,
+              "throughput_mpath_samples_per_s": sum(j["res"] ** 2 * j["spp"] for j in served_jobs) / served_span / 1e6}
+    st = srv.stats()
+    srv.close()
+
+    # plain: one job at a time through ar_render (first timed window's jobs)
+    plain_jobs = windows[W]
+    out = torch.empty(1024 * 1024 * 3, dtype=torch.float32, device="cuda")
+    stream_t = torch.cuda.current_stream()
+    flush.zero_()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream_t)
+    for i, job in enumerate(plain_jobs):
+        make_integrator(agentray, job, 10_000 * W + i).render(scenes[job["scene"]], cams[job["scene"]], job["res"],
+                                                              job["res"], out=out)
+    e1.record(stream_t)
+    torch.cuda.synchronize()
+    plain_ms = e0.elapsed_time(e1)
+    plain_value = sum(j["res"] ** 2 * j["spp"] for j in plain_jobs) / (plain_ms / 1e3) / 1e6
+    batched_first = sum(j["res"] ** 2 * j["spp"] for j in plain_jobs) / (ms_list[0] / 1e3) / 1e6
+
+    if rank == 0:
+        n_pt = sum(1 for w in windows[W:] for j in w if j["integrator"] == "pt")
+        line = {
+            "metric": METRIC, "value": value, "unit": "Mpath-samples/s", "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": total_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded procedural scenes and job stream)",
+            "config": {"workload": SERVED_DESC, "jobs_per_step": per, "timed_jobs": per * K,
+                       "timed_pt_jobs": n_pt, "stream_jobs": n_jobs, "l2": "flushed (256 MiB write) before each window",
+                       "parallelism": f"replicas x{world}", "server": {"path_capacity": 1 << 21,
+                                                                       "bdpt_batch_samples": 1 << 19}},
+            "e2e": {"value": e2e_value, "unit": "Mpath-samples/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": int(d2h / max(1, min(2, K))),
+                    "note": "scenes resident; per step the job descriptors go host->device and every image "
+                            "returns to a host buffer"},
+            "plain": {"value": plain_value, "unit": "Mpath-samples/s", "jobs": len(plain_jobs),
+                      "batched_same_jobs": batched_first, "speedup_batched_vs_plain": batched_first / plain_value,
+                      "equal_relmse": "same per-job sample keys: images equal up to atomic-add order "
+                                      "(tests/test_gpu_serving.py)"},
+            "served": served,
+            "server_stats": st,
+            "gpu_launches": int(st["pt_ticks"] * 5 + st["bdpt_batches"] * 20),
+            "clocks": clk.summary(),
+        }
+        line["roofline"] = served_roofline(args, ctx, agentray, S, scenes, cams, built, peaks, peak_kind, torch)
+        line["cpu_baseline"] = cpu_baseline_served(stream, built, n_samples_target=args.cpu_samples)
+        print(json.dumps(line), flush=True)
+
+
+def served_roofline(args, ctx, agentray, S, scenes, cams, built, peaks, peak_kind, torch):
+    """Per-launch timing of the dominant kernel (pt_extend) on the middle
+    scene (k=4, 139k tris) at 512x512 x 16 spp, with the reference-traversal
+    bytes model."""
+    k = 4
+    pt = agentray.PathTracer(agentray.PathTracerConfig(spp=16, max_depth=8, rr_depth=3, seed=3))
+    out = torch.empty(512 * 512 * 3, dtype=torch.float32, device="cuda")
+    pt.render(scenes[k], cams[k], 512, 512, out=out)
+    ctx.profile(True)
+    ctx.profile_reset()
+    for _ in range(2):
+        pt.render(scenes[k], cams[k], 512, 512, out=out)
+    torch.cuda.synchronize()
+    ctx.profile(False)
+    prof = ctx.profile_read()
+    stats = ctx.render_stats()
+    nodes, tris = reference_traversal_counts(built[k][0], cams[k])
+    b_ray = 32 + 16 + 32 * nodes + 36 * tris
+    ln, ms = prof.get("pt_extend", (1, 0.0))
+    rays_per_launch = stats["extend_rays"] / max(1, stats["extend_launches"])
+    avg_s = (ms / max(1, ln)) / 1e3
+    achieved = rays_per_launch * b_ray / avg_s / 1e9 if avg_s > 0 else 0.0
+    return {"bound": "hbm", "kernel": "pt_extend", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / peaks["hbm_gbs"], "traffic": profile_traffic("pt_extend_served4"),
+            "peak_kind": peak_kind,
+            "case": "served scene 4 (138,944 tris), 512x512, 16 spp, PT depth 8",
+            "bytes_model": f"rays/launch {rays_per_launch:.0f} x (48 + 32*{nodes:.2f} nodes + 36*{tris:.2f} tris) B; "
+                           f"reference-traversal counts",
+            "kernels_ms": {k2: {"launches": v[0], "ms": v[1]} for k2, v in prof.items()}}
+
+
+def cpu_jobs_sample(stream, n_samples_target):
+    """A bounded, representative sample of the stream for the CPU: the first
+    jobs of the stream, each rendered at 1 spp over its full resolution, until
+    about `n_samples_target` samples are covered."""
+    out, total = [], 0
+    for job in stream:
+        if total >= n_samples_target:
             break
-    dt = time.perf_counter() - t0
-    return {"value": reps * w * h * cfg.spp / dt / 1e6, "unit": "Mpath-samples/s", "cores": cores, "kind": "port",
-            "sample": f"{reps} full 256x256x16spp render(s) of the same scene, reference sampler, "
-                      f"{dt:.2f} s wall on {cores} threads"}
+        out.append(job)
+        total += job["res"] ** 2
+    return out
 
 
-def run_ours(args, rank, local, world):
-    import torch
+def cpu_render_rate(stream, built, n_samples_target, threads):
+    import oracle as O
+    jobs = cpu_jobs_sample(stream, n_samples_target)
+    cache = {}
+    samples, secs = 0, 0.0
+    for i, job in enumerate(jobs):
+        k = job["scene"]
+        if k not in cache:
+            cache[k] = O.OracleScene(built[k][0])
+        cfg = job_cfg(dict(job, spp=1), seed=i)
+        t0 = time.perf_counter()
+        cache[k].render(built[k][1], cfg, job["res"], job["res"], sampler=O.SAMPLER_XOSHIRO, threads=threads)
+        secs += time.perf_counter() - t0
+        samples += job["res"] ** 2
+    return samples / secs / 1e6, len(jobs), samples, secs
+
+
+def cpu_baseline_served(stream, built, n_samples_target):
+    cores = os.cpu_count() or 1
+    rate, n, samples, secs = cpu_render_rate(stream, built, n_samples_target, cores)
+    return {"value": rate, "unit": "Mpath-samples/s", "cores": cores, "kind": "port",
+            "sample": f"first {n} jobs of the stream at 1 spp (full resolution, same scene/integrator mix): "
+                      f"{samples} path samples in {secs:.1f} s on {cores} threads"}
+
+
+# ------------------------------------------------------------- pt_cornell ----
+def run_pt_cornell(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind, stream):
     import agentray
     import agentray.scenes as S
     from agentray import _abi as A
     from agentray.scene_data import integrator_cfg
 
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    peaks, peak_kind = load_peaks()
-    ctx = agentray.Context(local)
-    # A dedicated stream: the library launches on it, and every timing event is
-    # recorded on it (torch's legacy default stream has handle 0, which the C ABI
-    # reads as "use the context's own stream").
-    stream = torch.cuda.Stream()
-    torch.cuda.set_stream(stream)
-    ctx.set_stream(stream.cuda_stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    if args.workload == "bvh":
-        return run_bvh(args, rank, world, ctx, torch, flush, barrier, dist, peaks, peak_kind)
-
     sc, cam = S.cornell_box(1)
     W = H = 256
     spp = 16
-    cfg = integrator_cfg(A.INTEGRATOR_PT, spp=spp, max_depth=8, rr_depth=3, seed=rank)
     scene = agentray.Scene(ctx, sc)
     out = torch.empty(W * H * 3, dtype=torch.float32, device="cuda")
     pt = agentray.PathTracer(agentray.PathTracerConfig(spp=spp, max_depth=8, rr_depth=3, seed=rank))
@@ -246,7 +426,6 @@ def run_ours(args, rank, local, world):
         pt.render(scene, cam, W, H, out=out)
     torch.cuda.synchronize()
     barrier()
-    torch.cuda.synchronize()
     step_ms = []
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
@@ -259,11 +438,8 @@ def run_ours(args, rank, local, world):
             step_ms.append((e0, e1))
         torch.cuda.synchronize()
     st = ctx.render_stats()
-    # per render: `ticks` graph replays of (plan, generate, extend, shade, shadow)
     launches = args.steps * st["extend_launches"] * 5
     barrier()
-    # Instrumented pass (same workload, same number of renders): the stages are
-    # launched individually with CUDA events on the library stream.
     ctx.profile(True)
     ctx.profile_reset()
     for _ in range(args.steps):
@@ -280,8 +456,6 @@ def run_ours(args, rank, local, world):
     stats = ctx.render_stats()
     samples = W * H * spp
     value = world * samples * args.steps / (total_ms / 1e3) / 1e6
-
-    # end to end through the public API with host buffers
     e2e_ms = []
     host_out = np.empty(W * H * 3, np.float32)
     h2d = 0
@@ -297,65 +471,59 @@ def run_ours(args, rank, local, world):
         if i >= 2:
             e2e_ms.append(dt)
     e2e_value = samples / (statistics.mean(e2e_ms) / 1e3) / 1e6
-
-    line = None
     if rank == 0:
-        nodes, tris = reference_traversal_counts(sc, cam, W, H)
+        nodes, tris = reference_traversal_counts(sc, cam)
         b_ray = 32 + 16 + 32 * nodes + 36 * tris
         ln, ms = prof.get("pt_extend", (0, 0.0))
         rays_per_launch = stats["extend_rays"] / max(1, stats["extend_launches"])
         avg_s = (ms / max(1, ln)) / 1e3
         achieved = rays_per_launch * b_ray / avg_s / 1e9 if avg_s > 0 else 0.0
-        traffic = profile_traffic("pt_extend_cornell")
+        import oracle as O
+        osc = O.OracleScene(sc)
+        cfg = integrator_cfg(A.INTEGRATOR_PT, spp=16, max_depth=8, rr_depth=3)
+        cores = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        osc.render(cam, cfg, W, H, sampler=O.SAMPLER_XOSHIRO, threads=cores)
+        cpu_s = time.perf_counter() - t0
         line = {
             "metric": METRIC, "value": value, "unit": "Mpath-samples/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
             "config": {"workload": "pt_cornell: PT Cornell box 34 tris + quad light, 256x256, 16 spp, depth 8, RR 3",
-                       "width": W, "height": H, "spp": spp, "max_depth": 8, "rr_depth": 3,
                        "l2": "flushed (256 MiB write) before each timed step", "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e_value, "unit": "Mpath-samples/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": W * H * 3 * 4,
                     "includes": "Scene::new (host BVH build + upload) + render + readback"},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "kernel": "pt_extend", "achieved": achieved, "peak": peaks["hbm_gbs"],
-                         "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
-                         "peak_kind": peak_kind,
+                         "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                         "traffic": profile_traffic("pt_extend_cornell"), "peak_kind": peak_kind,
                          "bytes_model": f"rays/launch {rays_per_launch:.0f} x (48 + 32*{nodes:.2f} nodes + "
                                         f"36*{tris:.2f} tris) B; reference-traversal counts"},
             "kernels_ms": {k: {"launches": v[0], "ms": v[1]} for k, v in prof.items()},
-            "render_stats": stats,
-        }
-    clocks = clk.summary()
-    if rank == 0:
-        line["clocks"] = clocks
-        line["cpu_baseline"] = cpu_baseline_pt(sc, cam, integrator_cfg(A.INTEGRATOR_PT, spp=16, max_depth=8,
-                                                                       rr_depth=3))
+            "render_stats": stats, "clocks": clk.summary(),
+            "cpu_baseline": {"value": samples / cpu_s / 1e6, "unit": "Mpath-samples/s", "cores": cores,
+                             "kind": "port", "sample": "one full 256x256x16spp render, reference sampler"}}
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
 
 
-def run_bvh(args, rank, world, ctx, torch, flush, barrier, dist, peaks, peak_kind):
+# -------------------------------------------------------------------- bvh ----
+def run_bvh(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind, stream):
     import agentray
     import agentray.scenes as S
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     n_tris, n_rays = 1_000_000, 16_000_000
     sc = S.triangle_soup(n_tris, seed=2)
     scene = agentray.Scene(ctx, sc)
     ot, dt = S.soup_rays(n_rays, seed=3)
     ot_d = torch.from_numpy(ot).cuda()
     dt_d = torch.from_numpy(dt).cuda()
-    stream = torch.cuda.current_stream()
-    assert stream.cuda_stream != 0
     for _ in range(max(3, args.warmup)):
         scene.trace_closest(ot_d, dt_d)
     torch.cuda.synchronize()
-    ctx.profile(True)
-    ctx.profile_reset()
     barrier()
     ev = []
-    with ClockSampler(torch.cuda.current_device()) as clk:
+    with ClockSampler(local) as clk:
         for _ in range(args.steps):
             flush.zero_()
             a = torch.cuda.Event(enable_timing=True)
@@ -365,8 +533,6 @@ def run_bvh(args, rank, world, ctx, torch, flush, barrier, dist, peaks, peak_kin
             b.record(stream)
             ev.append((a, b))
         torch.cuda.synchronize()
-    ctx.profile(False)
-    prof = ctx.profile_read()
     total_ms = sum(a.elapsed_time(b) for a, b in ev)
     value = world * n_rays * args.steps / (total_ms / 1e3) / 1e6
     if rank == 0:
@@ -376,8 +542,7 @@ def run_bvh(args, rank, world, ctx, torch, flush, barrier, dist, peaks, peak_kin
         nodes = r["stats"]["nodes"] / 200_000
         tris = r["stats"]["tris"] / 200_000
         b_ray = 32 + 16 + 32 * nodes + 36 * tris
-        ln, ms = prof.get("trace_closest", (1, total_ms))
-        achieved = n_rays * b_ray / ((ms / ln) / 1e3) / 1e9
+        achieved = n_rays * b_ray / (total_ms / args.steps / 1e3) / 1e9
         t0 = time.perf_counter()
         osc.trace_closest(ot[:2_000_000], dt[:2_000_000])
         cpu = 2_000_000 / (time.perf_counter() - t0) / 1e6
@@ -394,9 +559,38 @@ def run_bvh(args, rank, world, ctx, torch, flush, barrier, dist, peaks, peak_kin
                 "cpu_baseline": {"value": cpu, "unit": "Mrays/s", "cores": os.cpu_count(), "kind": "port",
                                  "sample": "2M of the 16M rays, reference binary SAH traversal"}}
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+
+
+# -------------------------------------------------------------- reference ----
+def run_reference(args, rank, world):
+    """--impl reference: the reference CPU algorithms (oracle restatement with
+    the reference's xoshiro256++ per-pixel streams) on all host cores; each
+    step renders a bounded slice of the served stream (jobs at 1 spp over their
+    full resolution, ~args.cpu_samples samples per step)."""
+    if rank != 0:
+        return
+    import agentray.scenes as S
+    cores = os.cpu_count() or 1
+    stream = S.served_stream(args.jobs, seed=5)
+    built = [S.served_scene(k) for k in range(8)]
+    for w in range(args.warmup):
+        cpu_render_rate(stream[w * 3:], built, 16384, cores)
+    rates, tot_samples, tot_secs = [], 0, 0.0
+    for k in range(args.steps):
+        rate, n, samples, secs = cpu_render_rate(stream[k * 7:], built, args.cpu_samples // max(1, args.steps), cores)
+        tot_samples += samples
+        tot_secs += secs
+    value = tot_samples / tot_secs / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mpath-samples/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_secs / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded procedural scenes and job stream)",
+            "config": {"workload": SERVED_DESC},
+            "cpu_baseline": {"value": value, "unit": "Mpath-samples/s", "cores": cores, "kind": "port",
+                             "sample": f"{args.steps} slices of the stream, jobs at 1 spp over full resolution, "
+                                       f"{tot_samples} samples in {tot_secs:.1f} s"},
+            "e2e": {"value": value, "unit": "Mpath-samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
 
 
 def main():
@@ -405,13 +599,44 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="pt_cornell", choices=["pt_cornell", "bvh"])
+    ap.add_argument("--workload", default="served", choices=["served", "pt_cornell", "bvh"])
+    ap.add_argument("--jobs", type=int, default=2000)
+    ap.add_argument("--cpu-samples", dest="cpu_samples", type=int, default=4_000_000)
     args = ap.parse_args()
     rank, local, world = dist_env()
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
-    run_ours(args, rank, local, world)
+    import torch
+    import agentray
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    peaks, peak_kind = load_peaks()
+    ctx = agentray.Context(local)
+    # A dedicated stream: the library launches on it, and every timing event is
+    # recorded on it (torch's legacy default stream has handle 0, which the C ABI
+    # reads as "use the context's own stream").
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    if args.workload == "served":
+        run_served(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind)
+    elif args.workload == "pt_cornell":
+        run_pt_cornell(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind, stream)
+    else:
+        run_bvh(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind, stream)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 if __name__ == "__main__":

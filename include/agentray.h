@@ -297,10 +297,11 @@ int ar_server_create(ar_context* ctx, const ar_server_opts* opts, ar_server** ou
 /* Waits for admitted jobs to finish, then stops the worker. */
 int ar_server_destroy(ar_server* server);
 /* Non-blocking: queues the job and returns its id.  `scene` must stay alive
- * until the job finishes; `out_rgb` (host, W*H*3 floats) receives the image. */
+ * until the job finishes; `out_rgb` (W*H*3 floats; a device pointer on the
+ * server's device when out_on_device != 0, else host memory) receives the image. */
 int ar_job_submit(ar_server* server, const ar_scene* scene, const ar_camera_desc* camera,
                   const ar_integrator_cfg* cfg, uint32_t width, uint32_t height, float* out_rgb,
-                  uint64_t* job_id);
+                  uint32_t out_on_device, uint64_t* job_id);
 int ar_job_poll(ar_server* server, uint64_t job_id, ar_job_info* info);
 /* Blocks until the job leaves PENDING/RUNNING or timeout_ms passes
  * (AR_ERR_TIMEOUT). */
@@ -309,6 +310,9 @@ int ar_job_wait(ar_server* server, uint64_t job_id, double timeout_ms, ar_job_in
 int ar_job_cancel(ar_server* server, uint64_t job_id);
 int ar_server_get_stats(ar_server* server, ar_server_stats* out);
 double ar_server_now_ms(ar_server* server);
+/* Text summary of the worker's queues (pending / active / finishing jobs and
+ * their progress), for diagnostics. */
+int ar_server_debug_dump(ar_server* server, char* buf, uint32_t capacity);
 
 /* ---- instrumentation (no counterpart in the reference) ---- */
 

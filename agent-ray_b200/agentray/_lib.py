@@ -31,6 +31,8 @@ SIGNATURES = {
     "ar_poisson_reconstruct": (C.c_int, [C.c_void_p, C.POINTER(A.IntegratorCfg), C.c_uint32, C.c_uint32,
                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                          C.POINTER(C.c_double)]),
+    "ar_poisson_sor_static": (C.c_int, [C.POINTER(A.IntegratorCfg), C.c_uint32, C.c_uint32, C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ar_server_create": (C.c_int, [C.c_void_p, C.POINTER(A.ServerOpts), C.POINTER(C.c_void_p)]),
     "ar_server_destroy": (C.c_int, [C.c_void_p]),
     "ar_job_submit": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(A.CameraDesc), C.POINTER(A.IntegratorCfg),

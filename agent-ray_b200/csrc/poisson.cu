@@ -208,6 +208,21 @@ __global__ void k_cg_output(size_t n, const double* x, float* out) {
 
 }  // namespace
 
+// The red-black SOR solve with caller-provided scratch (rhs and img, 3*W*H
+// floats each) on `stream`; launches only, no allocation, no synchronisation.
+void poisson_sor_with_scratch(cudaStream_t stream, int num_sms, const ar_integrator_cfg& cfg, uint32_t w, uint32_t h,
+                              const float* primal, const float* gx, const float* gy, float* rhs, float* img,
+                              float* out) {
+    const size_t n = size_t(w) * h;
+    const int grid = std::max(1, std::min(int((n + 255) / 256), num_sms * 8));
+    k_rhs<<<grid, 256, 0, stream>>>(w, h, primal, gx, gy, cfg.alpha, rhs, img);
+    for (uint32_t it = 0; it < cfg.poisson_iterations; ++it)
+        for (uint32_t parity = 0; parity < 2; ++parity)
+            k_sor_half<<<grid, 256, 0, stream>>>(w, h, parity, rhs, img, cfg.alpha, cfg.sor_omega);
+    k_clamp<<<grid, 256, 0, stream>>>(3 * n, img, out);
+    AR_CUDA(cudaGetLastError());
+}
+
 void poisson_reconstruct(ar_context* ctx, const ar_integrator_cfg& cfg, uint32_t w, uint32_t h, const float* primal,
                          const float* gx, const float* gy, float* out, double* rel_residual) {
     const size_t n = size_t(w) * h;

@@ -253,6 +253,22 @@ int ar_poisson_reconstruct(ar_context* ctx, const ar_integrator_cfg* cfg, uint32
                            const float* primal, const float* grad_x, const float* grad_y, float* out,
                            uint32_t on_device, double* rel_residual);
 
+/* Scratch-free red-black SOR (no counterpart in the reference).  For callers
+ * that cannot allocate device memory while they run: a frame loop or a plugin
+ * whose host owns the device memory pool, or code between CUDA-graph captures
+ * where cudaMalloc would synchronise.  Same result as ar_poisson_reconstruct
+ * with AR_POISSON_SOR, but: all pointers are device pointers on the current
+ * device; work is queued on `cuda_stream` (NULL: the legacy default stream)
+ * without synchronising; no context is needed and nothing is allocated.  The
+ * solver's scratch is a static device array of 6 MiB that every GPU loading the
+ * library keeps until exit, which limits images to AR_STATIC_SOR_MAX_PIXELS
+ * pixels (larger ones fail with AR_ERR_INVALID_ARGUMENT).  The first call on a
+ * device looks the array up (do it before any stream capture); calls that
+ * overlap on the GPU share the array and race, so serialise them. */
+#define AR_STATIC_SOR_MAX_PIXELS (512u * 512u)
+int ar_poisson_sor_static(const ar_integrator_cfg* cfg, uint32_t width, uint32_t height, const float* primal,
+                          const float* grad_x, const float* grad_y, float* out, void* cuda_stream);
+
 /* ---- serving (no counterpart in the reference: it renders one job per call) ----
  * A server owns a worker thread that continuously batches every admitted job
  * into shared wavefront kernels: PT and GDPT paths stream through one path pool

@@ -9,6 +9,10 @@
 #include <cstdint>
 #include "ar_types.h"
 
+// Traversal kernels: 128 threads, at least 8 blocks per SM (<= 64 registers),
+// i.e. half the SM's warps resident to hide node-fetch latency.
+#define AR_TRAVERSAL_BOUNDS __launch_bounds__(128, 8)
+
 namespace ar {
 
 struct f3 {
@@ -136,6 +140,11 @@ __device__ __forceinline__ RayPre precompute(f3 o, f3 d, float tmin) {
 }
 
 __device__ __forceinline__ uint32_t byte_of(uint32_t w, uint32_t i) { return (w >> (8 * i)) & 0xffu; }
+// Byte i of w as a float, exactly: the bits 0x4B0000qq encode 2^23 + qq, and
+// subtracting 2^23 is exact (a byte-permute and an add instead of an I2F).
+__device__ __forceinline__ float byte_to_float(uint32_t w, uint32_t i) {
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7650u + i)) - 8388608.0f;
+}
 
 // Intersects the 8 children of node `ni`.  Outputs the node group (bits 8..15:
 // internal-child hits in traversal order i, bits 0..7: imask) and the leaf
@@ -170,12 +179,12 @@ __device__ __forceinline__ void intersect_node(const WideNode* nodes, uint32_t n
         const uint32_t nzw = nz ? hiz : loz, fzw = nz ? loz : hiz;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            const float tnx = fmaf(float(byte_of(nxw, j)), ax, bx);
-            const float tfx = fmaf(float(byte_of(fxw, j)), ax, bx);
-            const float tny = fmaf(float(byte_of(nyw, j)), ay, by);
-            const float tfy = fmaf(float(byte_of(fyw, j)), ay, by);
-            const float tnz = fmaf(float(byte_of(nzw, j)), az, bz);
-            const float tfz = fmaf(float(byte_of(fzw, j)), az, bz);
+            const float tnx = fmaf(byte_to_float(nxw, j), ax, bx);
+            const float tfx = fmaf(byte_to_float(fxw, j), ax, bx);
+            const float tny = fmaf(byte_to_float(nyw, j), ay, by);
+            const float tfy = fmaf(byte_to_float(fyw, j), ay, by);
+            const float tnz = fmaf(byte_to_float(nzw, j), az, bz);
+            const float tfz = fmaf(byte_to_float(fzw, j), az, bz);
             const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, r.tmin));
             const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tfar_limit));
             const uint32_t s = uint32_t(half * 4 + j);

@@ -110,6 +110,6 @@ struct DevScene {
 };
 
 constexpr uint32_t kInvalid = 0xFFFFFFFFu;
-constexpr int kTraversalStack = 64;
+constexpr int kTraversalStack = 32;
 
 }  // namespace ar

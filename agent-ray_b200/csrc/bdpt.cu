@@ -179,6 +179,64 @@ __device__ float mis_weight(const BdParams& P, const BdJob& J, uint32_t si, uint
     return float(1.0 / (1.0 + sum));
 }
 
+// Prefix form of the reference ratio walk for the power heuristic with
+// beta = 2 and no delta surface vertex (the only BSDFs here are Lambertian and
+// GGX).  With q_i = pdf_rev(z_i) / pdf_fwd(z_i) the camera-side terms of
+// strategy (s, t) are r1^2 (1 + q_{s-1}^2 + (q_{s-1} q_{s-2})^2 + ...), where
+// r1 = pdf_connect_cam / pdf_fwd(z_{s-1}); the bracket C_s obeys C_1 = 1,
+// C_s = 1 + q_{s-1}^2 C_{s-1}.  The light side is symmetric (D_t), and its
+// t = 1 term counts only for area lights.  Same sums as mis_weight, in FP64.
+constexpr uint32_t kMisCache = 16;
+struct MisCache {
+    double C[kMisCache], D[kMisCache];
+    float fwd_cam[kMisCache], fwd_light[kMisCache];
+    bool fast;
+};
+
+__device__ void build_mis_cache(const BdParams& P, const BdJob& J, uint32_t si, uint32_t S, uint32_t T, MisCache& mc) {
+    mc.fast = J.mis_mode == AR_MIS_POWER && J.mis_beta == 2.0f && S <= kMisCache && T <= kMisCache;
+    if (!mc.fast) return;
+    double c = 1.0;
+    for (uint32_t s = 1; s <= S; ++s) {
+        const Vtx v = load_vtx(P, 0, s - 1, si);
+        if (v.type == kTypeSurface && v.delta) mc.fast = false;
+        mc.fwd_cam[s - 1] = v.pdf_fwd;
+        if (s >= 2) {
+            const double q = double(fmaxf(v.pdf_rev, 0.f)) / double(fmaxf(v.pdf_fwd, 1e-30f));
+            c = 1.0 + q * q * c;
+        }
+        mc.C[s - 1] = c;  // C_s (s >= 1) with q_{s-1} taken from z[s-1]
+    }
+    double d = 1.0;
+    for (uint32_t t = 1; t <= T; ++t) {
+        const Vtx v = load_vtx(P, 1, t - 1, si);
+        if (v.type == kTypeSurface && v.delta) mc.fast = false;
+        mc.fwd_light[t - 1] = v.pdf_fwd;
+        if (t >= 2) {
+            const double q = double(fmaxf(v.pdf_rev, 0.f)) / double(fmaxf(v.pdf_fwd, 1e-30f));
+            d = 1.0 + q * q * d;
+        }
+        mc.D[t - 1] = d;
+    }
+}
+
+__device__ __forceinline__ float mis_weight_cached(const BdParams& P, const BdJob& J, const MisCache& mc, uint32_t si,
+                                                   uint32_t S, uint32_t T, uint32_t s, uint32_t t, float pdf_cc,
+                                                   float pdf_cl, bool light_is_point) {
+    if (!mc.fast) return mis_weight(P, J, si, S, T, s, t, pdf_cc, pdf_cl);
+    if (s + t == 2) return 1.0f;
+    double sum = 0.0;
+    if (s >= 2) {
+        const double r = double(pdf_cc) / double(fmaxf(mc.fwd_cam[s - 1], 1e-30f));
+        sum += r * r * mc.C[s - 1];
+    }
+    if (t >= 2 || (t == 1 && !light_is_point)) {
+        const double r = double(pdf_cl) / double(fmaxf(mc.fwd_light[t - 1], 1e-30f));
+        sum += r * r * mc.D[t - 1];
+    }
+    return float(1.0 / (1.0 + sum));
+}
+
 __device__ __forceinline__ void film_add(const BdJob& J, uint32_t pix, f3 v) {
     if (J.film64) {
         double* f = static_cast<double*>(J.film) + 3 * size_t(pix);
@@ -292,7 +350,7 @@ __global__ void __launch_bounds__(256) k_bd_generate(BdParams P) {
     }
 }
 
-__global__ void __launch_bounds__(128) k_bd_extend(BdParams P, uint32_t depth, int* err) {
+__global__ void AR_TRAVERSAL_BOUNDS k_bd_extend(BdParams P, uint32_t depth, int* err) {
     const uint32_t n = P.counts[depth];
     const int b = depth & 1;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
@@ -375,20 +433,39 @@ __global__ void __launch_bounds__(256) k_bd_vertex(BdParams P, uint32_t depth) {
 
 // connect_bdpt for s >= 2 (:782-1044) + the t == 0 extension.  Emits a shadow
 // ray with the MIS-weighted contribution, or deposits directly when t == 0.
+// Camera-side data of strategy (s, *): z = z[s-1] and its shading frame.
+struct CamSide {
+    Vtx z;
+    f3 zp_p;
+    Onb oz;
+    MatView mz;
+    f3 wo_zl;
+};
+
+__device__ __forceinline__ CamSide cam_side(const BdParams& P, const BdJob& J, uint32_t si, uint32_t s) {
+    CamSide c;
+    c.z = load_vtx(P, 0, s - 1, si);
+    c.zp_p = load_vtx(P, 0, s - 2, si).p;
+    c.oz = onb_from_normal(c.z.n);
+    c.mz = load_mat(J.sc, c.z.index);
+    c.wo_zl = to_local(c.oz, normalize(c.zp_p - c.z.p));
+    return c;
+}
+
 __device__ void connect_general(const BdParams& P, const BdJob& J, uint32_t job, uint32_t si, uint32_t S, uint32_t T,
-                                uint32_t s, uint32_t t, uint32_t pix) {
-    const Vtx z = load_vtx(P, 0, s - 1, si);
-    const Vtx zp = load_vtx(P, 0, s - 2, si);
+                                const MisCache& mc, bool lpt, const CamSide& cs, uint32_t s, uint32_t t,
+                                uint32_t pix) {
+    const Vtx& z = cs.z;
     if (t == 0) {
-        const MatView mz = load_mat(J.sc, z.index);
+        const MatView& mz = cs.mz;
         if (mz.emitter < 0 || !light_enabled(J.sc)) return;
         const LightView lt = load_light(J.sc, uint32_t(mz.emitter));
-        const f3 wo = normalize(zp.p - z.p);
+        const f3 wo = normalize(cs.zp_p - z.p);
         if (dot(lt.n, wo) <= 0.f) return;
         const f3 c = z.thr * lt.inten;
         if (max3(c) <= 0.f) return;
         const float pdf_cc = light_pmf_of(J.sc, uint32_t(mz.emitter)) / lt.area;
-        const float w = mis_weight(P, J, si, S, T, s, 0, pdf_cc, 0.f);
+        const float w = mis_weight_cached(P, J, mc, si, S, T, s, 0, pdf_cc, 0.f, lpt);
         film_add(J, pix, (c * w) * J.inv_spp);
         return;
     }
@@ -405,10 +482,9 @@ __device__ void connect_general(const BdParams& P, const BdJob& J, uint32_t job,
     const f3 sd = st - so;
     const float sdist = length(sd);
     if (sdist < 1e-6f) return;
-    const Onb oz = onb_from_normal(z.n);
-    const MatView mz = load_mat(J.sc, z.index);
-    const f3 wo_z = normalize(zp.p - z.p);
-    const f3 wo_zl = to_local(oz, wo_z);
+    const Onb& oz = cs.oz;
+    const MatView& mz = cs.mz;
+    const f3& wo_zl = cs.wo_zl;
     const f3 f_z = bsdf_eval(mz, to_local(oz, wi_z), wo_zl);
     if (is_zero(f_z)) return;
     f3 f_y = mk(1.f, 1.f, 1.f);
@@ -451,12 +527,12 @@ __device__ void connect_general(const BdParams& P, const BdJob& J, uint32_t job,
         pdf_cc = pdf_sa_to_area(bsdf_pdf(my, to_local(oy, wiy), wo_yl), y.p, z.p, z.n);
     }
     const float pdf_cl = pdf_sa_to_area(bsdf_pdf(mz, to_local(oz, normalize(y.p - z.p)), wo_zl), z.p, y.p, y.n);
-    const float w = mis_weight(P, J, si, S, T, s, t, pdf_cc, pdf_cl);
+    const float w = mis_weight_cached(P, J, mc, si, S, T, s, t, pdf_cc, pdf_cl, lpt);
     push_shadow(P, job, so, normalize(sd / sdist), sdist * (1.0f - 1e-4f), c * w, pix);
 }
 
 // connect_bdpt_s1 (:1051-1155): light tracing to the pinhole, splatted.
-__device__ void connect_s1(const BdParams& P, const BdJob& J, uint32_t job, uint32_t si, uint32_t S, uint32_t T,
+__device__ void connect_s1(const BdParams& P, const BdJob& J, uint32_t job, uint32_t si, uint32_t S, uint32_t T, const MisCache& mc, bool lpt,
                            uint32_t t) {
     const Vtx y = load_vtx(P, 1, t - 1, si);
     if (y.type == kTypeSurface && y.delta) return;
@@ -490,12 +566,14 @@ __device__ void connect_s1(const BdParams& P, const BdJob& J, uint32_t job, uint
     if (max3(c) <= 0.f) return;
     const Vtx z0 = load_vtx(P, 0, 0, si);
     const float pdf_cl = pdf_sa_to_area(bsdf_pdf(my, to_local(oy, wi), wo_yl), y.p, co, z0.n);
-    const float w = mis_weight(P, J, si, S, T, 1, t, 0.f, pdf_cl);
+    const float w = mis_weight_cached(P, J, mc, si, S, T, 1, t, 0.f, pdf_cl, lpt);
     const uint32_t ix = min(uint32_t(px), J.width - 1), iy = min(uint32_t(py), J.height - 1);
     const f3 o = y.p + (y.n * 1e-4f) * signum(dot(wi, y.n));
     push_shadow(P, job, o, normalize(wi), dist * (1.0f - 1e-4f), c * w, iy * J.width + ix);
 }
 
+// One thread per sample: the MIS prefix sums are built once, then the
+// strategies run camera-vertex-major so each z's frame is computed once.
 __global__ void __launch_bounds__(128) k_bd_connect(BdParams P) {
     for (uint32_t si = blockIdx.x * blockDim.x + threadIdx.x; si < P.nsamples; si += gridDim.x * blockDim.x) {
         const uint32_t job = P.sjob[si];
@@ -503,19 +581,20 @@ __global__ void __launch_bounds__(128) k_bd_connect(BdParams P) {
         const uint32_t S = P.nv[si], T = P.nv[P.nsamples + si];
         const uint32_t pix = uint32_t(P.sindex[si] % (J.width * J.height));
         const uint32_t limit = J.max_depth + 2;
-        for (uint32_t t = 0; t <= T; ++t)
-            for (uint32_t s = 1; s <= S; ++s) {
-                if (s + t < 2 || s + t > limit) continue;
-                if (s == 1) {
-                    if (t >= 2) connect_s1(P, J, job, si, S, T, t);
-                    continue;
-                }
-                connect_general(P, J, job, si, S, T, s, t, pix);
-            }
+        MisCache mc;
+        build_mis_cache(P, J, si, S, T, mc);
+        bool lpt = false;
+        if (T >= 1) lpt = J.sc.lights[load_vtx(P, 1, 0, si).index].kind == AR_LIGHT_POINT;
+        if (S >= 1)
+            for (uint32_t t = 2; t <= T && 1 + t <= limit; ++t) connect_s1(P, J, job, si, S, T, mc, lpt, t);
+        for (uint32_t s = 2; s <= S; ++s) {
+            const CamSide cs = cam_side(P, J, si, s);
+            for (uint32_t t = 0; t <= T && s + t <= limit; ++t) connect_general(P, J, job, si, S, T, mc, lpt, cs, s, t, pix);
+        }
     }
 }
 
-__global__ void __launch_bounds__(128) k_bd_shadow(BdParams P, int* err) {
+__global__ void AR_TRAVERSAL_BOUNDS k_bd_shadow(BdParams P, int* err) {
     const uint32_t n = min(P.counts[64], P.sh_cap);
     for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
         const float4 a = P.sh_o[m], d = P.sh_d[m];

@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(256) k_generate(EngineDev E, int q) {
     }
 }
 
-__global__ void __launch_bounds__(128) k_extend(EngineDev E, int q) {
+__global__ void AR_TRAVERSAL_BOUNDS k_extend(EngineDev E, int q) {
     const uint32_t n = E.cnt[q];
     const PathBuf B = E.buf[q];
     if (blockIdx.x == 0 && threadIdx.x == 0) E.stats[1] += n;
@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(256) k_shade(EngineDev E, int q) {
     }
 }
 
-__global__ void __launch_bounds__(128) k_shadow(EngineDev E, int q) {
+__global__ void AR_TRAVERSAL_BOUNDS k_shadow(EngineDev E, int q) {
     const uint32_t n = E.cnt[2];
     const PathBuf O = E.buf[q ^ 1];
     if (blockIdx.x == 0 && threadIdx.x == 0) E.stats[2] += n;

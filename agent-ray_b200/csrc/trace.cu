@@ -8,7 +8,7 @@ namespace ar {
 namespace {
 
 template <bool kAnyHit>
-__global__ void __launch_bounds__(128) trace_kernel(DevScene sc, const float4* __restrict__ org_tmin,
+__global__ void AR_TRAVERSAL_BOUNDS trace_kernel(DevScene sc, const float4* __restrict__ org_tmin,
                                                     const float4* __restrict__ dir_tmax, uint64_t n,
                                                     float4* __restrict__ hits, uint32_t* __restrict__ inst_ids,
                                                     uint8_t* __restrict__ occluded, int* err) {

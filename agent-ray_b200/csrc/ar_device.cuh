@@ -12,6 +12,8 @@
 // Traversal kernels: 128 threads, at least 8 blocks per SM (<= 64 registers),
 // i.e. half the SM's warps resident to hide node-fetch latency.
 #define AR_TRAVERSAL_BOUNDS __launch_bounds__(128, 8)
+// Resident blocks per SM under AR_TRAVERSAL_BOUNDS: the persistent grid of a ray-fetch launch.
+constexpr int kTraversalBlocksPerSm = 8;
 
 namespace ar {
 
@@ -345,6 +347,201 @@ __device__ bool traverse(const DevScene& sc, const Ray& world, HitRec& hit, int*
         visit = true;
     }
     return true;
+}
+
+// The same two-level traversal as traverse<>, restated as a resumable state
+// machine: start() loads a ray, step() performs one iteration (a node visit
+// with its leaf tests, or a stack pop) and returns true when the ray is done.
+// Kernels drive it with dynamic ray fetch (run_traversal below): a lane whose
+// ray finishes takes the next ray at once, so a warp is not held by its
+// slowest ray.
+template <bool kAnyHit>
+struct Traverser {
+    static constexpr uint32_t kNodeGroup = 0x80000000u, kMarker = 0x40000000u;
+    const DevScene* sc;
+    Ray world, local;
+    RayPre pre;
+    HitRec hit;
+    float ds, best_l, bu, bv;
+    uint32_t cur_inst, best_l_slot, node, guard;
+    uint2 group;
+    int sp;
+    bool in_blas, visit;
+    uint2 stack[kTraversalStack];
+
+    __device__ __forceinline__ void start(const DevScene* s, const Ray& r) {
+        sc = s;
+        world = r;
+        hit.t = r.tmax;
+        hit.slot = kInvalid;
+        hit.inst = kInvalid;
+        hit.u = hit.v = 0.f;
+        pre = precompute(r.o, r.d, r.tmin);
+        in_blas = false;
+        ds = 1.f;
+        cur_inst = kInvalid;
+        best_l = bu = bv = 0.f;
+        best_l_slot = kInvalid;
+        group = make_uint2(0, 0);
+        node = s->tlas_root;
+        visit = node != kInvalid;
+        sp = 0;
+        guard = 0;
+    }
+
+    // Returns true when the ray is finished (or failed: *err set).
+    __device__ __forceinline__ bool step(int* err) {
+        if (++guard > (1u << 22)) { atomicExch(err, 3); return true; }
+        if (visit) {
+            visit = false;
+            uint32_t cb, nbits, tbase, tbits;
+            intersect_node(sc->nodes, node, pre, in_blas ? best_l : hit.t, cb, nbits, tbase, tbits);
+            group = make_uint2(cb, nbits | kNodeGroup);
+            if (tbits) {
+                if (in_blas) {
+                    while (tbits) {
+                        const uint32_t b = __ffs(tbits) - 1;
+                        tbits &= tbits - 1;
+                        const TriRecord tr = load_tri(sc->tris, tbase + b);
+                        float t, u, v;
+                        if (tri_test(tr, local.o, local.d, local.tmin, best_l, t, u, v) && t < best_l) {
+                            if (kAnyHit) {
+                                if (__fdiv_rn(t, ds) < world.tmax) {
+                                    hit.t = t;
+                                    hit.slot = tbase + b;
+                                    hit.inst = cur_inst;
+                                    return true;
+                                }
+                            } else {
+                                best_l = t;
+                                best_l_slot = tbase + b;
+                                bu = u;
+                                bv = v;
+                            }
+                        }
+                    }
+                } else {
+                    if ((group.y >> 8) & 0xffu) {
+                        if (sp >= kTraversalStack) { atomicExch(err, 1); return true; }
+                        stack[sp++] = group;
+                    }
+                    group = make_uint2(0, 0);
+                    if (sp >= kTraversalStack) { atomicExch(err, 1); return true; }
+                    stack[sp++] = make_uint2(tbase, tbits);
+                }
+            }
+        }
+        if ((group.y & kNodeGroup) && ((group.y >> 8) & 0xffu)) {
+            const uint32_t hits = (group.y >> 8) & 0xffu;
+            const uint32_t i = __ffs(hits) - 1;
+            const uint32_t s = i ^ pre.oct;
+            const uint32_t imask = group.y & 0xffu;
+            node = group.x + __popc(imask & ((1u << s) - 1u));
+            group.y &= ~(1u << (8 + i));
+            if ((group.y >> 8) & 0xffu) {
+                if (sp >= kTraversalStack) { atomicExch(err, 1); return true; }
+                stack[sp++] = group;
+            }
+            group = make_uint2(0, 0);
+            visit = true;
+            return false;
+        }
+        if (sp == 0) return true;
+        const uint2 e = stack[--sp];
+        if (e.y & kNodeGroup) {
+            group = e;
+            return false;
+        }
+        if (e.y & kMarker) {
+            if (!kAnyHit && best_l_slot != kInvalid) {
+                const float tw = __fdiv_rn(best_l, ds);
+                if (tw < hit.t) {
+                    hit.t = tw;
+                    hit.slot = best_l_slot;
+                    hit.inst = cur_inst;
+                    hit.u = bu;
+                    hit.v = bv;
+                }
+            }
+            in_blas = false;
+            pre = precompute(world.o, world.d, world.tmin);
+            group = make_uint2(0, 0);
+            return false;
+        }
+        uint32_t bits = e.y;
+        const uint32_t b = __ffs(bits) - 1;
+        bits &= bits - 1;
+        if (bits) stack[sp++] = make_uint2(e.x, bits);
+        const InstanceRecord* ir = sc->instances + (e.x + b);
+        const float4* ip = reinterpret_cast<const float4*>(ir);
+        const float4 m0 = __ldg(ip), m1 = __ldg(ip + 1), m2 = __ldg(ip + 2);
+        const uint4 m3 = __ldg(reinterpret_cast<const uint4*>(ip + 3));
+        if (!m3.z) return false;
+        const f3 c0 = mk(m0.x, m0.y, m0.z), c1 = mk(m0.w, m1.x, m1.y), c2 = mk(m1.z, m1.w, m2.x),
+                 c3 = mk(m2.y, m2.z, m2.w);
+        const f3 lo = add_rn(c3, add_rn(add_rn(scale_rn(c0, world.o.x), scale_rn(c1, world.o.y)), scale_rn(c2, world.o.z)));
+        const f3 ldu = add_rn(add_rn(scale_rn(c0, world.d.x), scale_rn(c1, world.d.y)), scale_rn(c2, world.d.z));
+        const float scale = __fsqrt_rn(dot_rn(ldu, ldu));
+        if (scale < FLT_EPSILON) return false;
+        ds = scale;
+        local.o = lo;
+        local.d = normalize_rn(ldu);
+        local.tmin = __fmul_rn(world.tmin, ds);
+        best_l = __fmul_rn(kAnyHit ? world.tmax : hit.t, ds);
+        best_l_slot = kInvalid;
+        cur_inst = m3.y;
+        in_blas = true;
+        pre = precompute(local.o, local.d, local.tmin);
+        if (sp >= kTraversalStack) { atomicExch(err, 1); return true; }
+        stack[sp++] = make_uint2(0, kMarker);
+        node = m3.x;
+        visit = true;
+        return false;
+    }
+};
+
+// Persistent traversal with dynamic ray fetch.  Every lane of the warp calls
+// this (warp-uniform loop).  `counter` hands out ray indices in [0, n) (reset
+// to 0 before the launch); load(i, scene, ray) fetches ray i and its scene;
+// store(i, hit) writes the result.
+template <bool kAnyHit, class Load, class Store>
+__device__ __forceinline__ void run_traversal(uint32_t* counter, uint32_t n, int* err, Load load, Store store) {
+    Traverser<kAnyHit> tr;
+    int cur = -1;
+    bool more = true;
+    const uint32_t lane = threadIdx.x & 31u;
+    for (;;) {
+        const bool need = more && cur < 0;
+        const uint32_t mask = __ballot_sync(0xffffffffu, need);
+        if (mask) {
+            const int leader = __ffs(mask) - 1;
+            uint32_t base = 0;
+            if (int(lane) == leader) base = atomicAdd(counter, uint32_t(__popc(mask)));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (need) {
+                const uint32_t idx = base + __popc(mask & ((1u << lane) - 1u));
+                if (idx < n) {
+                    const DevScene* s;
+                    Ray r;
+                    load(idx, s, r);
+                    tr.start(s, r);
+                    cur = int(idx);
+                } else {
+                    more = false;
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, cur >= 0)) break;
+        if (cur >= 0) {
+            for (int k = 0; k < 16; ++k) {
+                if (tr.step(err)) {
+                    store(uint32_t(cur), tr.hit);
+                    cur = -1;
+                    break;
+                }
+            }
+        }
+    }
 }
 
 }  // namespace ar

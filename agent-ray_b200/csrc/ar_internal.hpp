@@ -123,6 +123,7 @@ struct ar_context {
     int num_sms = 0;
     ar::DevBuf err_flag;      // int: device-side error flag (stack overflow, budget)
     ar::DevBuf stats_d;       // uint64[8]: render work counters
+    ar::DevBuf fetch;         // uint32: ray-fetch cursor of the batched trace launches
     ar::Workspace work;       // wavefront state
     ar::Workspace io;         // staging for host <-> device transfers
     ar::Workspace films;      // accumulation films of the current render

@@ -35,6 +35,9 @@ namespace {
 
 constexpr uint32_t kTypeSurface = 0, kTypeCamera = 1, kTypeLight = 2;
 
+// Layout of the per-batch counter block (max_depth <= 62).
+constexpr uint32_t kBdShadowCursor = 127, kBdExtendCursor = 128, kBdCounts = 192;
+
 struct BdParams {
     const BdJob* jobs;
     const BdSegment* seg;
@@ -59,7 +62,8 @@ struct BdParams {
     float4* sh_c;  // contribution.xyz, pixel bits
     uint32_t* sh_job;
     uint32_t sh_cap;
-    uint32_t* counts;  // [0..63]: rays per bounce; [64]: shadow rays; [65]: overflow flag
+    uint32_t* counts;  // [0..63]: rays per bounce; [64]: shadow rays; [65]: overflow flag;
+                       // [kBdShadowCursor], [kBdExtendCursor + depth]: ray-fetch cursors
 };
 
 __device__ __forceinline__ size_t vidx(const BdParams& P, uint32_t sub, uint32_t k, uint32_t si) {
@@ -350,17 +354,20 @@ __global__ void __launch_bounds__(256) k_bd_generate(BdParams P) {
     }
 }
 
-__global__ void AR_TRAVERSAL_BOUNDS k_bd_extend(BdParams P, uint32_t depth, int* err) {
+__global__ void AR_TRAVERSAL_BOUNDS k_bd_extend(const __grid_constant__ BdParams P, uint32_t depth, int* err) {
     const uint32_t n = P.counts[depth];
     const int b = depth & 1;
-    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-        const float4 a = P.ray_o[b][j], d = P.ray_d[b][j];
-        const BdJob& J = P.jobs[P.sjob[P.qpath[b][j] >> 1]];
-        HitRec h;
-        traverse<false>(J.sc, Ray{mk(a.x, a.y, a.z), mk(d.x, d.y, d.z), a.w, d.w}, h, err);
-        P.hit[j] = make_float4(h.t, h.u, h.v, __uint_as_float(h.slot));
-        P.hit_inst[j] = h.inst;
-    }
+    run_traversal<false>(
+        &P.counts[kBdExtendCursor + depth], n, err,
+        [&](uint32_t j, const DevScene*& s, Ray& r) {
+            const float4 a = P.ray_o[b][j], d = P.ray_d[b][j];
+            s = &P.jobs[P.sjob[P.qpath[b][j] >> 1]].sc;
+            r = Ray{mk(a.x, a.y, a.z), mk(d.x, d.y, d.z), a.w, d.w};
+        },
+        [&](uint32_t j, const HitRec& h) {
+            P.hit[j] = make_float4(h.t, h.u, h.v, __uint_as_float(h.slot));
+            P.hit_inst[j] = h.inst;
+        });
 }
 
 // One bounce of both subpaths (:368-434, :498-556).
@@ -594,18 +601,22 @@ __global__ void __launch_bounds__(128) k_bd_connect(BdParams P) {
     }
 }
 
-__global__ void AR_TRAVERSAL_BOUNDS k_bd_shadow(BdParams P, int* err) {
+__global__ void AR_TRAVERSAL_BOUNDS k_bd_shadow(const __grid_constant__ BdParams P, int* err) {
     const uint32_t n = min(P.counts[64], P.sh_cap);
-    for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
-        const float4 a = P.sh_o[m], d = P.sh_d[m];
-        const BdJob& J = P.jobs[P.sh_job[m]];
-        HitRec h;
-        traverse<true>(J.sc, Ray{mk(a.x, a.y, a.z), mk(d.x, d.y, d.z), 0.f, d.w}, h, err);
-        if (h.slot == kInvalid) {
-            const float4 c = P.sh_c[m];
-            film_add(J, __float_as_uint(c.w), mk(c.x, c.y, c.z) * J.inv_spp);
-        }
-    }
+    run_traversal<true>(
+        &P.counts[kBdShadowCursor], n, err,
+        [&](uint32_t m, const DevScene*& s, Ray& r) {
+            const float4 a = P.sh_o[m], d = P.sh_d[m];
+            s = &P.jobs[P.sh_job[m]].sc;
+            r = Ray{mk(a.x, a.y, a.z), mk(d.x, d.y, d.z), 0.f, d.w};
+        },
+        [&](uint32_t m, const HitRec& h) {
+            if (h.slot == kInvalid) {
+                const BdJob& J = P.jobs[P.sh_job[m]];
+                const float4 c = P.sh_c[m];
+                film_add(J, __float_as_uint(c.w), mk(c.x, c.y, c.z) * J.inv_spp);
+            }
+        });
 }
 
 __global__ void k_bd_count(const uint32_t* counts, uint32_t max_depth, unsigned long long* stats, int* err) {
@@ -693,7 +704,7 @@ BdptBatcher* bdpt_create(ar_context* ctx, uint32_t max_depth_cap, uint32_t batch
     P.sh_d = carve<float4>(cur, P.sh_cap);
     P.sh_c = carve<float4>(cur, P.sh_cap);
     P.sh_job = carve<uint32_t>(cur, P.sh_cap);
-    P.counts = carve<uint32_t>(cur, 128);
+    P.counts = carve<uint32_t>(cur, kBdCounts);
     P.jobs = b->jobs_d.as<BdJob>();
     P.seg = b->seg_d.as<BdSegment>();
     return b.release();
@@ -734,7 +745,7 @@ void bdpt_run_batch(BdptBatcher* b, const std::vector<BdJob>& jobs, const std::v
     P.nsamples = nsamples;
     int* err = ctx->err_flag.as<int>();
     const int wide = ctx->num_sms * 8;
-    AR_CUDA(cudaMemsetAsync(P.counts, 0, 128 * sizeof(uint32_t), ctx->stream));
+    AR_CUDA(cudaMemsetAsync(P.counts, 0, kBdCounts * sizeof(uint32_t), ctx->stream));
     {
         KernelScope ks(ctx->prof, ctx->stream, "bdpt_generate");
         k_bd_generate<<<std::max(1, int(std::min<uint64_t>((2ull * nsamples + 255) / 256, wide))), 256, 0,
@@ -743,7 +754,7 @@ void bdpt_run_batch(BdptBatcher* b, const std::vector<BdJob>& jobs, const std::v
     for (uint32_t d = 0; d < max_depth; ++d) {
         {
             KernelScope ks(ctx->prof, ctx->stream, "bdpt_extend");
-            k_bd_extend<<<ctx->num_sms * 16, 128, 0, ctx->stream>>>(P, d, err);
+            k_bd_extend<<<ctx->num_sms * kTraversalBlocksPerSm, 128, 0, ctx->stream>>>(P, d, err);
         }
         {
             KernelScope ks(ctx->prof, ctx->stream, "bdpt_vertex");
@@ -757,7 +768,7 @@ void bdpt_run_batch(BdptBatcher* b, const std::vector<BdJob>& jobs, const std::v
     }
     {
         KernelScope ks(ctx->prof, ctx->stream, "bdpt_shadow");
-        k_bd_shadow<<<ctx->num_sms * 16, 128, 0, ctx->stream>>>(P, err);
+        k_bd_shadow<<<ctx->num_sms * kTraversalBlocksPerSm, 128, 0, ctx->stream>>>(P, err);
     }
     k_bd_count<<<1, 32, 0, ctx->stream>>>(P.counts, max_depth, ctx->stats_d.as<unsigned long long>(), err);
     AR_CUDA(cudaGetLastError());

@@ -44,6 +44,7 @@ ar_context* context_create_internal(int device) {
     AR_CUDA(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device));
     ctx->err_flag.alloc(64);
     AR_CUDA(cudaMemset(ctx->err_flag.ptr, 0, 64));
+    ctx->fetch.alloc(256);
     ctx->stats_d.alloc(8 * sizeof(uint64_t));
     AR_CUDA(cudaMemset(ctx->stats_d.ptr, 0, 8 * sizeof(uint64_t)));
     AR_CUDA(cudaMallocHost(&ctx->stats_h, 8 * sizeof(uint64_t)));

@@ -122,6 +122,8 @@ __global__ void k_plan(EngineDev E, int q) {
     E.cnt[q] = n_cont + used;
     E.cnt[q ^ 1] = 0;
     E.cnt[2] = 0;
+    E.cnt[8] = 0;  // ray-fetch cursors of the extend and shadow stages
+    E.cnt[9] = 0;
     E.stats[0] += used;
 }
 
@@ -163,23 +165,26 @@ __global__ void __launch_bounds__(256) k_generate(EngineDev E, int q) {
     }
 }
 
-__global__ void AR_TRAVERSAL_BOUNDS k_extend(EngineDev E, int q) {
+__global__ void AR_TRAVERSAL_BOUNDS k_extend(const __grid_constant__ EngineDev E, int q) {
     const uint32_t n = E.cnt[q];
     const PathBuf B = E.buf[q];
     if (blockIdx.x == 0 && threadIdx.x == 0) E.stats[1] += n;
-    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-        const uint4 kk = B.key[j];
-        HitRec h;
-        h.slot = kInvalid;
-        h.inst = kInvalid;
-        h.t = h.u = h.v = 0.f;
-        if (!(kk.w & kDead)) {
-            const float4 a = B.ray_o[j], b = B.ray_d[j];
-            traverse<false>(E.jobs[kk.x].sc, Ray{mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w}, h, E.err);
-        }
-        E.hit[j] = make_float4(h.t, h.u, h.v, __uint_as_float(h.slot));
-        E.hit_inst[j] = h.inst;
-    }
+    run_traversal<false>(
+        &E.cnt[8], n, E.err,
+        [&](uint32_t j, const DevScene*& s, Ray& r) {
+            const uint4 kk = B.key[j];
+            s = &E.jobs[kk.x].sc;
+            if (kk.w & kDead) {
+                r = Ray{mk(0.f, 0.f, 0.f), mk(0.f, 0.f, 1.f), 1.f, 0.f};  // empty t-range: a miss
+            } else {
+                const float4 a = B.ray_o[j], b = B.ray_d[j];
+                r = Ray{mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w};
+            }
+        },
+        [&](uint32_t j, const HitRec& h) {
+            E.hit[j] = make_float4(h.t, h.u, h.v, __uint_as_float(h.slot));
+            E.hit_inst[j] = h.inst;
+        });
 }
 
 __global__ void __launch_bounds__(256) k_shade(EngineDev E, int q) {
@@ -311,30 +316,34 @@ __global__ void __launch_bounds__(256) k_shade(EngineDev E, int q) {
     }
 }
 
-__global__ void AR_TRAVERSAL_BOUNDS k_shadow(EngineDev E, int q) {
+__global__ void AR_TRAVERSAL_BOUNDS k_shadow(const __grid_constant__ EngineDev E, int q) {
     const uint32_t n = E.cnt[2];
     const PathBuf O = E.buf[q ^ 1];
     if (blockIdx.x == 0 && threadIdx.x == 0) E.stats[2] += n;
-    for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
-        const float4 a = E.sh_o[m], b = E.sh_d[m];
-        const uint4 sk = E.sh_key[m];
-        HitRec h;
-        traverse<true>(E.jobs[sk.x].sc, Ray{mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w}, h, E.err);
-        const float4 c = E.sh_c[m];
-        const bool visible = h.slot == kInvalid;
-        if (__float_as_uint(c.w) & 1u) {
-            const float4 l = E.sh_L[m];
-            f3 L = mk(l.x, l.y, l.z);
-            if (visible) L = L + mk(c.x, c.y, c.z);
-            deposit(E, sk.x, sk.y, sk.z, L);
-        } else if (visible) {
-            float4 r = O.rad[sk.w];
-            r.x += c.x;
-            r.y += c.y;
-            r.z += c.z;
-            O.rad[sk.w] = r;
-        }
-    }
+    run_traversal<true>(
+        &E.cnt[9], n, E.err,
+        [&](uint32_t m, const DevScene*& s, Ray& r) {
+            const float4 a = E.sh_o[m], b = E.sh_d[m];
+            s = &E.jobs[E.sh_key[m].x].sc;
+            r = Ray{mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w};
+        },
+        [&](uint32_t m, const HitRec& h) {
+            const uint4 sk = E.sh_key[m];
+            const float4 c = E.sh_c[m];
+            const bool visible = h.slot == kInvalid;
+            if (__float_as_uint(c.w) & 1u) {
+                const float4 l = E.sh_L[m];
+                f3 L = mk(l.x, l.y, l.z);
+                if (visible) L = L + mk(c.x, c.y, c.z);
+                deposit(E, sk.x, sk.y, sk.z, L);
+            } else if (visible) {
+                float4 r = O.rad[sk.w];
+                r.x += c.x;
+                r.y += c.y;
+                r.z += c.z;
+                O.rad[sk.w] = r;
+            }
+        });
 }
 
 template <class T>
@@ -371,9 +380,9 @@ struct PathEngine {
         const int wide = ctx->num_sms * 8;
         k_plan<<<1, 32, 0, s>>>(E, q);
         k_generate<<<wide, 256, 0, s>>>(E, q);
-        k_extend<<<ctx->num_sms * 16, 128, 0, s>>>(E, q);
+        k_extend<<<ctx->num_sms * kTraversalBlocksPerSm, 128, 0, s>>>(E, q);
         k_shade<<<wide, 256, 0, s>>>(E, q);
-        k_shadow<<<ctx->num_sms * 16, 128, 0, s>>>(E, q);
+        k_shadow<<<ctx->num_sms * kTraversalBlocksPerSm, 128, 0, s>>>(E, q);
     }
 
     void build_graphs() {
@@ -497,9 +506,9 @@ void engine_tick(PathEngine* e) {
         const int wide = ctx->num_sms * 8;
         { KernelScope k(ctx->prof, s, "pt_plan"); k_plan<<<1, 32, 0, s>>>(e->E, q); }
         { KernelScope k(ctx->prof, s, "pt_generate"); k_generate<<<wide, 256, 0, s>>>(e->E, q); }
-        { KernelScope k(ctx->prof, s, "pt_extend"); k_extend<<<ctx->num_sms * 16, 128, 0, s>>>(e->E, q); }
+        { KernelScope k(ctx->prof, s, "pt_extend"); k_extend<<<ctx->num_sms * kTraversalBlocksPerSm, 128, 0, s>>>(e->E, q); }
         { KernelScope k(ctx->prof, s, "pt_shade"); k_shade<<<wide, 256, 0, s>>>(e->E, q); }
-        { KernelScope k(ctx->prof, s, "pt_shadow"); k_shadow<<<ctx->num_sms * 16, 128, 0, s>>>(e->E, q); }
+        { KernelScope k(ctx->prof, s, "pt_shadow"); k_shadow<<<ctx->num_sms * kTraversalBlocksPerSm, 128, 0, s>>>(e->E, q); }
         AR_CUDA(cudaGetLastError());
     } else {
         if (e->captured_stream != ctx->stream) e->build_graphs();

@@ -416,8 +416,16 @@ def run_pt_cornell(args, rank, local, world, torch, ctx, barrier, dist, peaks, p
     from agentray.scene_data import integrator_cfg
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    sc, cam = S.cornell_box(1)
-    W = H = 256
+    if args.workload == "pt_served4":
+        sc, cam = S.served_scene(4)
+        W = H = 512
+        desc = "pt_served4: PT on served scene 4 (138,944 tris, 335 instances, 2 quad lights), 512x512, 16 spp, depth 8"
+        prof_name = "pt_extend_served4"
+    else:
+        sc, cam = S.cornell_box(1)
+        W = H = 256
+        desc = "pt_cornell: PT Cornell box 34 tris + quad light, 256x256, 16 spp, depth 8, RR 3"
+        prof_name = "pt_extend_cornell"
     spp = 16
     scene = agentray.Scene(ctx, sc)
     out = torch.empty(W * H * 3, dtype=torch.float32, device="cuda")
@@ -489,7 +497,7 @@ def run_pt_cornell(args, rank, local, world, torch, ctx, barrier, dist, peaks, p
             "metric": METRIC, "value": value, "unit": "Mpath-samples/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
-            "config": {"workload": "pt_cornell: PT Cornell box 34 tris + quad light, 256x256, 16 spp, depth 8, RR 3",
+            "config": {"workload": desc,
                        "l2": "flushed (256 MiB write) before each timed step", "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e_value, "unit": "Mpath-samples/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": W * H * 3 * 4,
@@ -497,13 +505,13 @@ def run_pt_cornell(args, rank, local, world, torch, ctx, barrier, dist, peaks, p
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "kernel": "pt_extend", "achieved": achieved, "peak": peaks["hbm_gbs"],
                          "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
-                         "traffic": profile_traffic("pt_extend_cornell"), "peak_kind": peak_kind,
+                         "traffic": profile_traffic(prof_name), "peak_kind": peak_kind,
                          "bytes_model": f"rays/launch {rays_per_launch:.0f} x (48 + 32*{nodes:.2f} nodes + "
                                         f"36*{tris:.2f} tris) B; reference-traversal counts"},
             "kernels_ms": {k: {"launches": v[0], "ms": v[1]} for k, v in prof.items()},
             "render_stats": stats, "clocks": clk.summary(),
             "cpu_baseline": {"value": samples / cpu_s / 1e6, "unit": "Mpath-samples/s", "cores": cores,
-                             "kind": "port", "sample": "one full 256x256x16spp render, reference sampler"}}
+                             "kind": "port", "sample": f"one full {W}x{H}x{spp}spp render, reference sampler"}}
         print(json.dumps(line), flush=True)
 
 
@@ -599,7 +607,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="served", choices=["served", "pt_cornell", "bvh"])
+    ap.add_argument("--workload", default="served", choices=["served", "pt_cornell", "pt_served4", "bvh"])
     ap.add_argument("--jobs", type=int, default=2000)
     ap.add_argument("--cpu-samples", dest="cpu_samples", type=int, default=4_000_000)
     args = ap.parse_args()
@@ -630,7 +638,7 @@ def main():
 
     if args.workload == "served":
         run_served(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind)
-    elif args.workload == "pt_cornell":
+    elif args.workload in ("pt_cornell", "pt_served4"):
         run_pt_cornell(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind, stream)
     else:
         run_bvh(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind, stream)

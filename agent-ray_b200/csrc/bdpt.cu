@@ -35,8 +35,11 @@ namespace {
 
 constexpr uint32_t kTypeSurface = 0, kTypeCamera = 1, kTypeLight = 2;
 
-// Layout of the per-batch counter block (max_depth <= 62).
-constexpr uint32_t kBdShadowCursor = 127, kBdExtendCursor = 128, kBdCounts = 192;
+// Layout of the per-batch counter block (max_depth <= 62): rays per bounce,
+// shadow count and overflow flag, ray-fetch cursors, then the histogram and
+// bucket offsets of the (S, T) sort.
+constexpr uint32_t kBdShadowCursor = 127, kBdExtendCursor = 128, kBdBins = 256, kBdHist = 192,
+                   kBdOffs = kBdHist + kBdBins, kBdCounts = kBdOffs + kBdBins;
 
 struct BdParams {
     const BdJob* jobs;
@@ -63,7 +66,9 @@ struct BdParams {
     uint32_t* sh_job;
     uint32_t sh_cap;
     uint32_t* counts;  // [0..63]: rays per bounce; [64]: shadow rays; [65]: overflow flag;
-                       // [kBdShadowCursor], [kBdExtendCursor + depth]: ray-fetch cursors
+                       // [kBdShadowCursor], [kBdExtendCursor + depth]: ray-fetch cursors;
+                       // [kBdHist..], [kBdOffs..]: (S, T) histogram and bucket offsets
+    uint32_t* order;   // batch samples sorted by (S, T)
 };
 
 __device__ __forceinline__ size_t vidx(const BdParams& P, uint32_t sub, uint32_t k, uint32_t si) {
@@ -128,7 +133,7 @@ __device__ __forceinline__ f3 uniform_sphere(float ux, float uy) {
 __device__ __forceinline__ bool mis_delta(const Vtx& v) { return v.type == kTypeSurface && v.delta; }
 
 // mis_weight (:594-770) with the area-light extension for the t == 1 step.
-__device__ float mis_weight(const BdParams& P, const BdJob& J, uint32_t si, uint32_t S, uint32_t T, uint32_t s,
+__device__ __noinline__ float mis_weight(const BdParams& P, const BdJob& J, uint32_t si, uint32_t S, uint32_t T, uint32_t s,
                             uint32_t t, float pdf_cc, float pdf_cl) {
     if (J.mis_mode == AR_MIS_UNIFORM) {
         const uint32_t len = s + t;
@@ -438,6 +443,12 @@ __global__ void __launch_bounds__(256) k_bd_vertex(BdParams P, uint32_t depth) {
     }
 }
 
+// Out-of-line BSDF bodies for the connection kernel: its warps diverge
+// across strategies, and one copy of each body keeps the instruction
+// footprint small.  Same arithmetic as the inline forms.
+__device__ __noinline__ f3 bsdf_eval_ool(const MatView& m, f3 wi, f3 wo) { return bsdf_eval(m, wi, wo); }
+__device__ __noinline__ float bsdf_pdf_ool(const MatView& m, f3 wi, f3 wo) { return bsdf_pdf(m, wi, wo); }
+
 // connect_bdpt for s >= 2 (:782-1044) + the t == 0 extension.  Emits a shadow
 // ray with the MIS-weighted contribution, or deposits directly when t == 0.
 // Camera-side data of strategy (s, *): z = z[s-1] and its shading frame.
@@ -492,7 +503,7 @@ __device__ void connect_general(const BdParams& P, const BdJob& J, uint32_t job,
     const Onb& oz = cs.oz;
     const MatView& mz = cs.mz;
     const f3& wo_zl = cs.wo_zl;
-    const f3 f_z = bsdf_eval(mz, to_local(oz, wi_z), wo_zl);
+    const f3 f_z = bsdf_eval_ool(mz, to_local(oz, wi_z), wo_zl);
     if (is_zero(f_z)) return;
     f3 f_y = mk(1.f, 1.f, 1.f);
     Onb oy;
@@ -503,7 +514,7 @@ __device__ void connect_general(const BdParams& P, const BdJob& J, uint32_t job,
         my = load_mat(J.sc, y.index);
         const Vtx yp = load_vtx(P, 1, t - 2, si);
         wo_yl = to_local(oy, normalize(yp.p - y.p));
-        f_y = bsdf_eval(my, to_local(oy, wi_y), wo_yl);
+        f_y = bsdf_eval_ool(my, to_local(oy, wi_y), wo_yl);
     }
     if (is_zero(f_y)) return;
     const float g = geometry_term(z.p, z.n, y.p, y.n);
@@ -515,7 +526,7 @@ __device__ void connect_general(const BdParams& P, const BdJob& J, uint32_t job,
             f3 lwi, lrad;
             float ldist, lpdf;
             if (!light_sample(L, z.p, 0.f, 0.f, lwi, ldist, lrad, lpdf)) return;
-            const f3 f_direct = bsdf_eval(mz, to_local(oz, lwi), wo_zl);
+            const f3 f_direct = bsdf_eval_ool(mz, to_local(oz, lwi), wo_zl);
             c = ((z.thr * f_direct) * fabsf(dot(z.n, lwi))) * lrad;
         } else {
             if (dot(y.n, wi_y) <= 0.f) return;
@@ -531,9 +542,9 @@ __device__ void connect_general(const BdParams& P, const BdJob& J, uint32_t job,
         pdf_cc = pdf_sa_to_area(light_pdf_emission_dir(L, normalize(z.p - y.p)), y.p, z.p, z.n);
     } else {
         const f3 wiy = normalize(z.p - y.p);
-        pdf_cc = pdf_sa_to_area(bsdf_pdf(my, to_local(oy, wiy), wo_yl), y.p, z.p, z.n);
+        pdf_cc = pdf_sa_to_area(bsdf_pdf_ool(my, to_local(oy, wiy), wo_yl), y.p, z.p, z.n);
     }
-    const float pdf_cl = pdf_sa_to_area(bsdf_pdf(mz, to_local(oz, normalize(y.p - z.p)), wo_zl), z.p, y.p, y.n);
+    const float pdf_cl = pdf_sa_to_area(bsdf_pdf_ool(mz, to_local(oz, normalize(y.p - z.p)), wo_zl), z.p, y.p, y.n);
     const float w = mis_weight_cached(P, J, mc, si, S, T, s, t, pdf_cc, pdf_cl, lpt);
     push_shadow(P, job, so, normalize(sd / sdist), sdist * (1.0f - 1e-4f), c * w, pix);
 }
@@ -566,23 +577,74 @@ __device__ void connect_s1(const BdParams& P, const BdJob& J, uint32_t job, uint
     const MatView my = load_mat(J.sc, y.index);
     const Vtx yp = load_vtx(P, 1, t - 2, si);
     const f3 wo_yl = to_local(oy, normalize(yp.p - y.p));
-    const f3 f_y = bsdf_eval(my, to_local(oy, wi), wo_yl);
+    const f3 f_y = bsdf_eval_ool(my, to_local(oy, wi), wo_yl);
     if (is_zero(f_y)) return;
     const float gf = fabsf(dot(y.n, wi)) / (dist * dist);
     const f3 c = ((y.thr * f_y) * gf) * we;
     if (max3(c) <= 0.f) return;
     const Vtx z0 = load_vtx(P, 0, 0, si);
-    const float pdf_cl = pdf_sa_to_area(bsdf_pdf(my, to_local(oy, wi), wo_yl), y.p, co, z0.n);
+    const float pdf_cl = pdf_sa_to_area(bsdf_pdf_ool(my, to_local(oy, wi), wo_yl), y.p, co, z0.n);
     const float w = mis_weight_cached(P, J, mc, si, S, T, 1, t, 0.f, pdf_cl, lpt);
     const uint32_t ix = min(uint32_t(px), J.width - 1), iy = min(uint32_t(py), J.height - 1);
     const f3 o = y.p + (y.n * 1e-4f) * signum(dot(wi, y.n));
     push_shadow(P, job, o, normalize(wi), dist * (1.0f - 1e-4f), c * w, iy * J.width + ix);
 }
 
+// Counting sort of the batch samples by their subpath lengths (S, T), so the
+// warps of the connection kernel run strategy loops of equal trip counts.
+__device__ __forceinline__ uint32_t bd_sort_key(const BdParams& P, uint32_t si) {
+    const uint32_t S = P.nv[si], T = P.nv[P.nsamples + si];
+    return min(S, 15u) * 16u + min(T, 15u);
+}
+
+__global__ void __launch_bounds__(256) k_bd_hist(BdParams P) {
+    __shared__ uint32_t h[kBdBins];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t si = blockIdx.x * 256 + threadIdx.x;
+    if (si < P.nsamples) atomicAdd(&h[bd_sort_key(P, si)], 1u);
+    __syncthreads();
+    if (h[threadIdx.x]) atomicAdd(&P.counts[kBdHist + threadIdx.x], h[threadIdx.x]);
+}
+
+__global__ void __launch_bounds__(256) k_bd_scan(BdParams P) {
+    __shared__ uint32_t h[kBdBins];
+    h[threadIdx.x] = P.counts[kBdHist + threadIdx.x];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t acc = 0;
+        for (uint32_t k = 0; k < kBdBins; ++k) {
+            const uint32_t c = h[k];
+            h[k] = acc;
+            acc += c;
+        }
+    }
+    __syncthreads();
+    P.counts[kBdOffs + threadIdx.x] = h[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(256) k_bd_scatter(BdParams P) {
+    __shared__ uint32_t h[kBdBins], base[kBdBins];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t si = blockIdx.x * 256 + threadIdx.x;
+    const bool live = si < P.nsamples;
+    uint32_t key = 0, rank = 0;
+    if (live) {
+        key = bd_sort_key(P, si);
+        rank = atomicAdd(&h[key], 1u);
+    }
+    __syncthreads();
+    if (h[threadIdx.x]) base[threadIdx.x] = atomicAdd(&P.counts[kBdOffs + threadIdx.x], h[threadIdx.x]);
+    __syncthreads();
+    if (live) P.order[base[key] + rank] = si;
+}
+
 // One thread per sample: the MIS prefix sums are built once, then the
 // strategies run camera-vertex-major so each z's frame is computed once.
 __global__ void __launch_bounds__(128) k_bd_connect(BdParams P) {
-    for (uint32_t si = blockIdx.x * blockDim.x + threadIdx.x; si < P.nsamples; si += gridDim.x * blockDim.x) {
+    for (uint32_t oi = blockIdx.x * blockDim.x + threadIdx.x; oi < P.nsamples; oi += gridDim.x * blockDim.x) {
+        const uint32_t si = P.order[oi];
         const uint32_t job = P.sjob[si];
         const BdJob& J = P.jobs[job];
         const uint32_t S = P.nv[si], T = P.nv[P.nsamples + si];
@@ -662,7 +724,7 @@ struct BdptBatcher {
 size_t bdpt_batch_bytes(uint32_t max_depth, uint32_t batch) {
     const size_t maxv = max_depth + 1;
     const size_t per_sample = 2 * maxv * 48 + 2 + 2 * (16 + 4) + 2 * 2 * (32 + 4) + 2 * 20 + 4 + 8 +
-                              size_t(max_pairs_for(max_depth)) * 52;
+                              size_t(max_pairs_for(max_depth)) * 52 + 4;
     return per_sample * batch + 64 * 1024;
 }
 
@@ -705,6 +767,7 @@ BdptBatcher* bdpt_create(ar_context* ctx, uint32_t max_depth_cap, uint32_t batch
     P.sh_c = carve<float4>(cur, P.sh_cap);
     P.sh_job = carve<uint32_t>(cur, P.sh_cap);
     P.counts = carve<uint32_t>(cur, kBdCounts);
+    P.order = carve<uint32_t>(cur, batch);
     P.jobs = b->jobs_d.as<BdJob>();
     P.seg = b->seg_d.as<BdSegment>();
     return b.release();
@@ -760,6 +823,13 @@ void bdpt_run_batch(BdptBatcher* b, const std::vector<BdJob>& jobs, const std::v
             KernelScope ks(ctx->prof, ctx->stream, "bdpt_vertex");
             k_bd_vertex<<<wide, 256, 0, ctx->stream>>>(P, d);
         }
+    }
+    {
+        KernelScope ks(ctx->prof, ctx->stream, "bdpt_sort");
+        const int g = std::max(1, int((nsamples + 255) / 256));
+        k_bd_hist<<<g, 256, 0, ctx->stream>>>(P);
+        k_bd_scan<<<1, 256, 0, ctx->stream>>>(P);
+        k_bd_scatter<<<g, 256, 0, ctx->stream>>>(P);
     }
     {
         KernelScope ks(ctx->prof, ctx->stream, "bdpt_connect");

@@ -11,9 +11,12 @@
 
 // Traversal kernels: 128 threads, at least 8 blocks per SM (<= 64 registers),
 // i.e. half the SM's warps resident to hide node-fetch latency.
-#define AR_TRAVERSAL_BOUNDS __launch_bounds__(128, 8)
+#ifndef AR_TRAVERSAL_MIN_BLOCKS
+#define AR_TRAVERSAL_MIN_BLOCKS 8
+#endif
+#define AR_TRAVERSAL_BOUNDS __launch_bounds__(128, AR_TRAVERSAL_MIN_BLOCKS)
 // Resident blocks per SM under AR_TRAVERSAL_BOUNDS: the persistent grid of a ray-fetch launch.
-constexpr int kTraversalBlocksPerSm = 8;
+constexpr int kTraversalBlocksPerSm = AR_TRAVERSAL_MIN_BLOCKS;
 
 namespace ar {
 
@@ -133,9 +136,9 @@ __device__ __forceinline__ RayPre precompute(f3 o, f3 d, float tmin) {
     RayPre r;
     r.o = o;
     const float eps = 1e-20f;
-    r.inv.x = 1.0f / (fabsf(d.x) > eps ? d.x : copysignf(eps, d.x));
-    r.inv.y = 1.0f / (fabsf(d.y) > eps ? d.y : copysignf(eps, d.y));
-    r.inv.z = 1.0f / (fabsf(d.z) > eps ? d.z : copysignf(eps, d.z));
+    r.inv.x = __frcp_rn(fabsf(d.x) > eps ? d.x : copysignf(eps, d.x));
+    r.inv.y = __frcp_rn(fabsf(d.y) > eps ? d.y : copysignf(eps, d.y));
+    r.inv.z = __frcp_rn(fabsf(d.z) > eps ? d.z : copysignf(eps, d.z));
     r.oct = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
     r.tmin = tmin;
     return r;
@@ -206,155 +209,14 @@ __device__ __forceinline__ void intersect_node(const WideNode* nodes, uint32_t n
 }
 
 // Two-level closest-hit / any-hit traversal (TLAS::intersect + BLASAccel::intersect,
-// src/accel/bvh.rs:247-296, :413-447).  One stack serves both levels: entering
-// an instance pushes a marker so that popping it restores the world ray.
-// Returns false (and flags *err) on stack overflow.
-template <bool kAnyHit>
-__device__ bool traverse(const DevScene& sc, const Ray& world, HitRec& hit, int* err) {
-    hit.t = world.tmax;
-    hit.slot = kInvalid;
-    hit.inst = kInvalid;
-    hit.u = hit.v = 0.f;
-    if (sc.tlas_root == kInvalid) return true;
-
-    uint2 stack[kTraversalStack];
-    int sp = 0;
-    const uint32_t kNodeGroup = 0x80000000u, kMarker = 0x40000000u;
-
-    RayPre pre = precompute(world.o, world.d, world.tmin);
-    bool in_blas = false;
-    Ray local;
-    float ds = 1.f;
-    uint32_t cur_inst = kInvalid;
-    float best_l = 0.f, bu = 0.f, bv = 0.f;
-    uint32_t best_l_slot = kInvalid;
-
-    uint2 group = make_uint2(0, 0);  // current node group
-    uint32_t node = sc.tlas_root;
-    bool visit = true;
-    // Bounded loop: a well-formed tree ends far earlier; a corrupt one sets the
-    // error flag instead of spinning.
-    for (uint32_t guard = 0;; ++guard) {
-        if (guard > (1u << 22)) { atomicExch(err, 3); return false; }
-        if (visit) {
-            visit = false;
-            uint32_t cb, nbits, tbase, tbits;
-            intersect_node(sc.nodes, node, pre, in_blas ? best_l : hit.t, cb, nbits, tbase, tbits);
-            group = make_uint2(cb, nbits | kNodeGroup);
-            if (tbits) {
-                if (in_blas) {
-                    while (tbits) {
-                        const uint32_t b = __ffs(tbits) - 1;
-                        tbits &= tbits - 1;
-                        const TriRecord tr = load_tri(sc.tris, tbase + b);
-                        float t, u, v;
-                        if (tri_test(tr, local.o, local.d, local.tmin, best_l, t, u, v) && t < best_l) {
-                            if (kAnyHit) {
-                                if (__fdiv_rn(t, ds) < world.tmax) {
-                                    hit.t = t;
-                                    hit.slot = tbase + b;
-                                    hit.inst = cur_inst;
-                                    return true;
-                                }
-                            } else {
-                                best_l = t;
-                                best_l_slot = tbase + b;
-                                bu = u;
-                                bv = v;
-                            }
-                        }
-                    }
-                } else {
-                    // TLAS leaves: resume the node group after the instances.
-                    if ((group.y >> 8) & 0xffu) {
-                        if (sp >= kTraversalStack) { atomicExch(err, 1); return false; }
-                        stack[sp++] = group;
-                    }
-                    group = make_uint2(0, 0);
-                    if (sp >= kTraversalStack) { atomicExch(err, 1); return false; }
-                    stack[sp++] = make_uint2(tbase, tbits);  // leaf group (instances)
-                }
-            }
-        }
-        // Choose the next node from the current group, else pop.
-        if ((group.y & kNodeGroup) && ((group.y >> 8) & 0xffu)) {
-            const uint32_t hits = (group.y >> 8) & 0xffu;
-            const uint32_t i = __ffs(hits) - 1;
-            const uint32_t s = i ^ pre.oct;
-            const uint32_t imask = group.y & 0xffu;
-            node = group.x + __popc(imask & ((1u << s) - 1u));
-            group.y &= ~(1u << (8 + i));
-            if ((group.y >> 8) & 0xffu) {
-                if (sp >= kTraversalStack) { atomicExch(err, 1); return false; }
-                stack[sp++] = group;
-            }
-            group = make_uint2(0, 0);
-            visit = true;
-            continue;
-        }
-        if (sp == 0) break;
-        uint2 e = stack[--sp];
-        if (e.y & kNodeGroup) {
-            group = e;
-            continue;
-        }
-        if (e.y & kMarker) {
-            // Leave the instance: convert the local best back to world t.
-            if (!kAnyHit && best_l_slot != kInvalid) {
-                const float tw = __fdiv_rn(best_l, ds);
-                if (tw < hit.t) {
-                    hit.t = tw;
-                    hit.slot = best_l_slot;
-                    hit.inst = cur_inst;
-                    hit.u = bu;
-                    hit.v = bv;
-                }
-            }
-            in_blas = false;
-            pre = precompute(world.o, world.d, world.tmin);
-            group = make_uint2(0, 0);
-            continue;
-        }
-        // Instance leaf group: enter the next instance.
-        uint32_t bits = e.y;
-        const uint32_t b = __ffs(bits) - 1;
-        bits &= bits - 1;
-        if (bits) stack[sp++] = make_uint2(e.x, bits);
-        const InstanceRecord* ir = sc.instances + (e.x + b);
-        const float4* ip = reinterpret_cast<const float4*>(ir);
-        const float4 m0 = __ldg(ip), m1 = __ldg(ip + 1), m2 = __ldg(ip + 2);
-        const uint4 m3 = __ldg(reinterpret_cast<const uint4*>(ip + 3));
-        if (!m3.z) continue;  // mesh without triangles
-        const f3 c0 = mk(m0.x, m0.y, m0.z), c1 = mk(m0.w, m1.x, m1.y), c2 = mk(m1.z, m1.w, m2.x),
-                 c3 = mk(m2.y, m2.z, m2.w);
-        // glam transform_point3a / transform_vector3a: ((c0*x + c1*y) + c2*z) + c3
-        const f3 lo = add_rn(c3, add_rn(add_rn(scale_rn(c0, world.o.x), scale_rn(c1, world.o.y)), scale_rn(c2, world.o.z)));
-        const f3 ldu = add_rn(add_rn(scale_rn(c0, world.d.x), scale_rn(c1, world.d.y)), scale_rn(c2, world.d.z));
-        const float scale = __fsqrt_rn(dot_rn(ldu, ldu));
-        if (scale < FLT_EPSILON) continue;
-        ds = scale;
-        local.o = lo;
-        local.d = normalize_rn(ldu);
-        local.tmin = __fmul_rn(world.tmin, ds);
-        best_l = __fmul_rn(kAnyHit ? world.tmax : hit.t, ds);
-        best_l_slot = kInvalid;
-        cur_inst = m3.y;
-        in_blas = true;
-        pre = precompute(local.o, local.d, local.tmin);
-        if (sp >= kTraversalStack) { atomicExch(err, 1); return false; }
-        stack[sp++] = make_uint2(0, kMarker);
-        node = m3.x;
-        visit = true;
-    }
-    return true;
-}
-
-// The same two-level traversal as traverse<>, restated as a resumable state
-// machine: start() loads a ray, step() performs one iteration (a node visit
-// with its leaf tests, or a stack pop) and returns true when the ray is done.
-// Kernels drive it with dynamic ray fetch (run_traversal below): a lane whose
-// ray finishes takes the next ray at once, so a warp is not held by its
-// slowest ray.
+// src/accel/bvh.rs:247-296, :413-447) as a resumable state machine.  One
+// stack serves both levels: entering an instance pushes a marker so that
+// popping it restores the world ray.  start() loads a ray, step() performs one
+// iteration (a node visit with its leaf tests, or a stack pop) and returns
+// true when the ray is done; stack overflow or a runaway loop sets *err and
+// ends the ray.  Kernels drive it with dynamic ray fetch (run_traversal
+// below): a lane whose ray finishes takes the next ray at once, so a warp is
+// not held by its slowest ray.
 template <bool kAnyHit>
 struct Traverser {
     static constexpr uint32_t kNodeGroup = 0x80000000u, kMarker = 0x40000000u;
@@ -367,7 +229,6 @@ struct Traverser {
     uint2 group;
     int sp;
     bool in_blas, visit;
-    uint2 stack[kTraversalStack];
 
     __device__ __forceinline__ void start(const DevScene* s, const Ray& r) {
         sc = s;
@@ -390,7 +251,9 @@ struct Traverser {
     }
 
     // Returns true when the ray is finished (or failed: *err set).
-    __device__ __forceinline__ bool step(int* err) {
+    // `stack` is the caller's local array (kept out of the struct so that the
+    // scalar state stays in registers).
+    __device__ __forceinline__ bool step(int* err, uint2* stack) {
         if (++guard > (1u << 22)) { atomicExch(err, 3); return true; }
         if (visit) {
             visit = false;
@@ -507,6 +370,7 @@ struct Traverser {
 template <bool kAnyHit, class Load, class Store>
 __device__ __forceinline__ void run_traversal(uint32_t* counter, uint32_t n, int* err, Load load, Store store) {
     Traverser<kAnyHit> tr;
+    uint2 stack[kTraversalStack];
     int cur = -1;
     bool more = true;
     const uint32_t lane = threadIdx.x & 31u;
@@ -534,7 +398,7 @@ __device__ __forceinline__ void run_traversal(uint32_t* counter, uint32_t n, int
         if (!__any_sync(0xffffffffu, cur >= 0)) break;
         if (cur >= 0) {
             for (int k = 0; k < 16; ++k) {
-                if (tr.step(err)) {
+                if (tr.step(err, stack)) {
                     store(uint32_t(cur), tr.hit);
                     cur = -1;
                     break;

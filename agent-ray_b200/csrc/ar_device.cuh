@@ -15,6 +15,10 @@
 #define AR_TRAVERSAL_MIN_BLOCKS 8
 #endif
 #define AR_TRAVERSAL_BOUNDS __launch_bounds__(128, AR_TRAVERSAL_MIN_BLOCKS)
+// Traversal steps a lane runs between two ray-fetch rounds of its warp.
+#ifndef AR_TRAVERSAL_STEPS
+#define AR_TRAVERSAL_STEPS 4
+#endif
 // Resident blocks per SM under AR_TRAVERSAL_BOUNDS: the persistent grid of a ray-fetch launch.
 constexpr int kTraversalBlocksPerSm = AR_TRAVERSAL_MIN_BLOCKS;
 
@@ -212,8 +216,8 @@ __device__ __forceinline__ void intersect_node(const WideNode* nodes, uint32_t n
 // src/accel/bvh.rs:247-296, :413-447) as a resumable state machine.  One
 // stack serves both levels: entering an instance pushes a marker so that
 // popping it restores the world ray.  start() loads a ray, step() performs one
-// iteration (a node visit with its leaf tests, or a stack pop) and returns
-// true when the ray is done; stack overflow or a runaway loop sets *err and
+// node visit with its leaf tests and the stack work up to the next node, and
+// returns true when the ray is done; stack overflow or a runaway loop sets *err and
 // ends the ray.  Kernels drive it with dynamic ray fetch (run_traversal
 // below): a lane whose ray finishes takes the next ray at once, so a warp is
 // not held by its slowest ray.
@@ -250,13 +254,14 @@ struct Traverser {
         guard = 0;
     }
 
-    // Returns true when the ray is finished (or failed: *err set).
-    // `stack` is the caller's local array (kept out of the struct so that the
-    // scalar state stays in registers).
+    // One step = one node visit (with its leaf tests) followed by the stack
+    // work that leads to the next node to visit, so every active lane of a
+    // warp intersects a node in every step.  Returns true when the ray is
+    // finished (or failed: *err set).  `stack` is the caller's local array
+    // (kept out of the struct so that the scalar state stays in registers).
     __device__ __forceinline__ bool step(int* err, uint2* stack) {
         if (++guard > (1u << 22)) { atomicExch(err, 3); return true; }
         if (visit) {
-            visit = false;
             uint32_t cb, nbits, tbase, tbits;
             intersect_node(sc->nodes, node, pre, in_blas ? best_l : hit.t, cb, nbits, tbase, tbits);
             group = make_uint2(cb, nbits | kNodeGroup);
@@ -284,82 +289,95 @@ struct Traverser {
                         }
                     }
                 } else {
+                    // TLAS leaves: resume the node group after the instances.
                     if ((group.y >> 8) & 0xffu) {
                         if (sp >= kTraversalStack) { atomicExch(err, 1); return true; }
                         stack[sp++] = group;
                     }
                     group = make_uint2(0, 0);
                     if (sp >= kTraversalStack) { atomicExch(err, 1); return true; }
-                    stack[sp++] = make_uint2(tbase, tbits);
+                    stack[sp++] = make_uint2(tbase, tbits);  // leaf group (instances)
                 }
             }
         }
-        if ((group.y & kNodeGroup) && ((group.y >> 8) & 0xffu)) {
-            const uint32_t hits = (group.y >> 8) & 0xffu;
-            const uint32_t i = __ffs(hits) - 1;
-            const uint32_t s = i ^ pre.oct;
-            const uint32_t imask = group.y & 0xffu;
-            node = group.x + __popc(imask & ((1u << s) - 1u));
-            group.y &= ~(1u << (8 + i));
-            if ((group.y >> 8) & 0xffu) {
-                if (sp >= kTraversalStack) { atomicExch(err, 1); return true; }
-                stack[sp++] = group;
+        // Find the next node: the nearest child of the current group, else
+        // pop (node groups, instance exits and entries) until one is found.
+        // Every pass pops one entry, so the loop ends within sp passes.
+        for (;;) {
+            if ((group.y & kNodeGroup) && ((group.y >> 8) & 0xffu)) {
+                const uint32_t hits = (group.y >> 8) & 0xffu;
+                const uint32_t i = __ffs(hits) - 1;
+                const uint32_t s = i ^ pre.oct;
+                const uint32_t imask = group.y & 0xffu;
+                node = group.x + __popc(imask & ((1u << s) - 1u));
+                group.y &= ~(1u << (8 + i));
+                if ((group.y >> 8) & 0xffu) {
+                    if (sp >= kTraversalStack) { atomicExch(err, 1); return true; }
+                    stack[sp++] = group;
+                }
+                group = make_uint2(0, 0);
+                visit = true;
+                return false;
+            }
+            if (sp == 0) {
+                visit = false;
+                return true;
+            }
+            const uint2 e = stack[--sp];
+            if (e.y & kNodeGroup) {
+                group = e;
+                continue;
             }
             group = make_uint2(0, 0);
+            if (e.y & kMarker) {
+                // Leave the instance: convert the local best back to world t.
+                if (!kAnyHit && best_l_slot != kInvalid) {
+                    const float tw = __fdiv_rn(best_l, ds);
+                    if (tw < hit.t) {
+                        hit.t = tw;
+                        hit.slot = best_l_slot;
+                        hit.inst = cur_inst;
+                        hit.u = bu;
+                        hit.v = bv;
+                    }
+                }
+                in_blas = false;
+                pre = precompute(world.o, world.d, world.tmin);
+                continue;
+            }
+            // Instance leaf group: enter the next instance.
+            uint32_t bits = e.y;
+            const uint32_t b = __ffs(bits) - 1;
+            bits &= bits - 1;
+            if (bits) stack[sp++] = make_uint2(e.x, bits);
+            const InstanceRecord* ir = sc->instances + (e.x + b);
+            const float4* ip = reinterpret_cast<const float4*>(ir);
+            const float4 m0 = __ldg(ip), m1 = __ldg(ip + 1), m2 = __ldg(ip + 2);
+            const uint4 m3 = __ldg(reinterpret_cast<const uint4*>(ip + 3));
+            if (!m3.z) continue;  // mesh without triangles
+            const f3 c0 = mk(m0.x, m0.y, m0.z), c1 = mk(m0.w, m1.x, m1.y), c2 = mk(m1.z, m1.w, m2.x),
+                     c3 = mk(m2.y, m2.z, m2.w);
+            // glam transform_point3a / transform_vector3a: ((c0*x + c1*y) + c2*z) + c3
+            const f3 lo =
+                add_rn(c3, add_rn(add_rn(scale_rn(c0, world.o.x), scale_rn(c1, world.o.y)), scale_rn(c2, world.o.z)));
+            const f3 ldu = add_rn(add_rn(scale_rn(c0, world.d.x), scale_rn(c1, world.d.y)), scale_rn(c2, world.d.z));
+            const float scale = __fsqrt_rn(dot_rn(ldu, ldu));
+            if (scale < FLT_EPSILON) continue;
+            ds = scale;
+            local.o = lo;
+            local.d = normalize_rn(ldu);
+            local.tmin = __fmul_rn(world.tmin, ds);
+            best_l = __fmul_rn(kAnyHit ? world.tmax : hit.t, ds);
+            best_l_slot = kInvalid;
+            cur_inst = m3.y;
+            in_blas = true;
+            pre = precompute(local.o, local.d, local.tmin);
+            if (sp >= kTraversalStack) { atomicExch(err, 1); return true; }
+            stack[sp++] = make_uint2(0, kMarker);
+            node = m3.x;
             visit = true;
             return false;
         }
-        if (sp == 0) return true;
-        const uint2 e = stack[--sp];
-        if (e.y & kNodeGroup) {
-            group = e;
-            return false;
-        }
-        if (e.y & kMarker) {
-            if (!kAnyHit && best_l_slot != kInvalid) {
-                const float tw = __fdiv_rn(best_l, ds);
-                if (tw < hit.t) {
-                    hit.t = tw;
-                    hit.slot = best_l_slot;
-                    hit.inst = cur_inst;
-                    hit.u = bu;
-                    hit.v = bv;
-                }
-            }
-            in_blas = false;
-            pre = precompute(world.o, world.d, world.tmin);
-            group = make_uint2(0, 0);
-            return false;
-        }
-        uint32_t bits = e.y;
-        const uint32_t b = __ffs(bits) - 1;
-        bits &= bits - 1;
-        if (bits) stack[sp++] = make_uint2(e.x, bits);
-        const InstanceRecord* ir = sc->instances + (e.x + b);
-        const float4* ip = reinterpret_cast<const float4*>(ir);
-        const float4 m0 = __ldg(ip), m1 = __ldg(ip + 1), m2 = __ldg(ip + 2);
-        const uint4 m3 = __ldg(reinterpret_cast<const uint4*>(ip + 3));
-        if (!m3.z) return false;
-        const f3 c0 = mk(m0.x, m0.y, m0.z), c1 = mk(m0.w, m1.x, m1.y), c2 = mk(m1.z, m1.w, m2.x),
-                 c3 = mk(m2.y, m2.z, m2.w);
-        const f3 lo = add_rn(c3, add_rn(add_rn(scale_rn(c0, world.o.x), scale_rn(c1, world.o.y)), scale_rn(c2, world.o.z)));
-        const f3 ldu = add_rn(add_rn(scale_rn(c0, world.d.x), scale_rn(c1, world.d.y)), scale_rn(c2, world.d.z));
-        const float scale = __fsqrt_rn(dot_rn(ldu, ldu));
-        if (scale < FLT_EPSILON) return false;
-        ds = scale;
-        local.o = lo;
-        local.d = normalize_rn(ldu);
-        local.tmin = __fmul_rn(world.tmin, ds);
-        best_l = __fmul_rn(kAnyHit ? world.tmax : hit.t, ds);
-        best_l_slot = kInvalid;
-        cur_inst = m3.y;
-        in_blas = true;
-        pre = precompute(local.o, local.d, local.tmin);
-        if (sp >= kTraversalStack) { atomicExch(err, 1); return true; }
-        stack[sp++] = make_uint2(0, kMarker);
-        node = m3.x;
-        visit = true;
-        return false;
     }
 };
 
@@ -397,7 +415,7 @@ __device__ __forceinline__ void run_traversal(uint32_t* counter, uint32_t n, int
         }
         if (!__any_sync(0xffffffffu, cur >= 0)) break;
         if (cur >= 0) {
-            for (int k = 0; k < 16; ++k) {
+            for (int k = 0; k < AR_TRAVERSAL_STEPS; ++k) {
                 if (tr.step(err, stack)) {
                     store(uint32_t(cur), tr.hit);
                     cur = -1;

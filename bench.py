@@ -1,7 +1,8 @@
 """Benchmark driver: one JSON line on rank 0.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload served|pt_cornell|bvh] [--jobs J]
+                    [--workload served|pt_cornell|pt_served4|bvh] [--jobs J]
+                    [--window-jobs J] [--served-jobs J]
 
 Workloads (seeded synthetic inputs with the stated shapes; no dataset exists):
   served      (default) the served batched-rendering stream: Poisson arrivals of
@@ -9,16 +10,19 @@ Workloads (seeded synthetic inputs with the stated shapes; no dataset exists):
               10k-1M triangles, resolution from {128,256,512,1024}^2, spp from
               {4,16,64}, PT or BDPT 70/30 (PT: depth 8, RR from 3; BDPT: depth
               8, RR from 3, power-heuristic MIS).  Metric: Mpath-samples/s.
-              A step is one window of J/(W+K) consecutive jobs submitted to the
-              render server together (continuous batching under a backlog);
+              A step is one window of --window-jobs (16) consecutive jobs of
+              the stream submitted to the render server together (continuous
+              batching under a backlog);
               `value` is the throughput of the K timed windows with images kept
               on the GPU, `e2e` the same windows' jobs with images returned to
               pinned host buffers.  `served` adds p50/p99 latency of a Poisson
-              arrival run at 80% of the measured capacity, and `plain` the
+              arrival run at 80% of the measured capacity over the next
+              --served-jobs (160) jobs of the stream, and `plain` the
               one-job-at-a-time GPU path (ar_render per job) on the first timed
               window's jobs.
   pt_cornell  PT Cornell box (34 tris + quad light, 256x256, 16 spp, depth 8);
               one step = one full render.
+  pt_served4  PT on served scene 4 (139k tris, 335 instances), 512x512, 16 spp.
   bvh         BVH micro-benchmark: 1M triangles, 16M closest-hit rays (Mrays/s).
 
 Timing: CUDA events on the stream the library launches on (pt_cornell, bvh)
@@ -204,10 +208,9 @@ def run_served(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_
     srv = agentray.Server(ctx, film_budget_bytes=24 << 30, path_capacity=1 << 21, bdpt_batch_samples=1 << 19,
                           bdpt_max_depth=8)
     W, K = max(3, args.warmup), args.steps
-    n_burst = int(n_jobs * 0.6)
-    per = max(1, n_burst // (W + K))
+    per = max(1, min(args.window_jobs, n_jobs // (W + K + 1)))
     windows = [stream[i * per:(i + 1) * per] for i in range(W + K)]
-    served_jobs = stream[(W + K) * per:]
+    served_jobs = stream[(W + K) * per:(W + K) * per + args.served_jobs]
     side = torch.cuda.Stream()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     dev_out = {128: [], 256: [], 512: [], 1024: []}
@@ -318,7 +321,9 @@ def run_served(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_
             "ms_per_step": total_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded procedural scenes and job stream)",
             "config": {"workload": SERVED_DESC, "jobs_per_step": per, "timed_jobs": per * K,
-                       "timed_pt_jobs": n_pt, "stream_jobs": n_jobs, "l2": "flushed (256 MiB write) before each window",
+                       "timed_pt_jobs": n_pt, "stream_jobs": n_jobs,
+                       "stream_use": f"jobs [0, {(W + K) * per}) as W+K windows of {per}, the next "
+                                     f"{len(served_jobs)} as the Poisson-arrival served run", "l2": "flushed (256 MiB write) before each window",
                        "parallelism": f"replicas x{world}", "server": {"path_capacity": 1 << 21,
                                                                        "bdpt_batch_samples": 1 << 19}},
             "e2e": {"value": e2e_value, "unit": "Mpath-samples/s", "h2d_bytes_per_step": 0,
@@ -609,6 +614,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="served", choices=["served", "pt_cornell", "pt_served4", "bvh"])
     ap.add_argument("--jobs", type=int, default=2000)
+    ap.add_argument("--window-jobs", dest="window_jobs", type=int, default=16)
+    ap.add_argument("--served-jobs", dest="served_jobs", type=int, default=160)
     ap.add_argument("--cpu-samples", dest="cpu_samples", type=int, default=4_000_000)
     args = ap.parse_args()
     rank, local, world = dist_env()

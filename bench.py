@@ -1,7 +1,8 @@
 """Benchmark driver: one JSON line on rank 0.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload served|pt_cornell|pt_served4|bvh] [--jobs J]
+                    [--workload served|pt_cornell|pt_served4|bdpt_room|gdpt_room|bvh]
+                    [--jobs J]
                     [--window-jobs J] [--served-jobs J]
 
 Workloads (seeded synthetic inputs with the stated shapes; no dataset exists):
@@ -23,6 +24,8 @@ Workloads (seeded synthetic inputs with the stated shapes; no dataset exists):
   pt_cornell  PT Cornell box (34 tris + quad light, 256x256, 16 spp, depth 8);
               one step = one full render.
   pt_served4  PT on served scene 4 (139k tris, 335 instances), 512x512, 16 spp.
+  bdpt_room   BDPT on the 200k-tri room, 512x512, 64 spp, depth 10, FP64 film.
+  gdpt_room   GDPT on the room, 1024x1024, 32 spp, CG Poisson to 1e-6.
   bvh         BVH micro-benchmark: 1M triangles, 16M closest-hit rays (Mrays/s).
 
 Timing: CUDA events on the stream the library launches on (pt_cornell, bvh)
@@ -294,6 +297,7 @@ def run_served(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_
               "mean_ms": float(lat.mean()) if len(lat) else None,
               "throughput_mpath_samples_per_s": sum(j["res"] ** 2 * j["spp"] for j in served_jobs) / served_span / 1e6}
     st = srv.stats()
+    relmse = served_relmse(agentray, srv, scenes, cams, stream)
     srv.close()
 
     # plain: one job at a time through ar_render (first timed window's jobs)
@@ -335,6 +339,7 @@ def run_served(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_
                       "equal_relmse": "same per-job sample keys: images equal up to atomic-add order "
                                       "(tests/test_gpu_serving.py)"},
             "served": served,
+            "relmse": relmse,
             "server_stats": st,
             "gpu_launches": int(st["pt_ticks"] * 5 + st["bdpt_batches"] * 20),
             "clocks": clk.summary(),
@@ -342,6 +347,44 @@ def run_served(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_
         line["roofline"] = served_roofline(args, ctx, agentray, S, scenes, cams, built, peaks, peak_kind, torch)
         line["cpu_baseline"] = cpu_baseline_served(stream, built, n_samples_target=args.cpu_samples)
         print(json.dumps(line), flush=True)
+
+
+def served_relmse(agentray, srv, scenes, cams, stream):
+    """relMSE (mean of (x - ref)^2 / (ref^2 + 1e-2)) of a PT and a BDPT job,
+    rendered by the server inside a mix of stream jobs and by the plain path,
+    against an FP64-film 2048-spp render of the same scene (tests pin the GPU's
+    relMSE to the FP64 CPU oracle's).  Scene 0, 128x128, 16 spp, depth 8."""
+    from agentray import _abi as A
+    k, r, spp = 0, 128, 16
+
+    def rel(x, ref):
+        return float(np.mean((x.astype(np.float64) - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+    out = {}
+    mix = [j for j in stream[:64] if j["res"] <= 512][:6]
+    for name, cls, cfg_cls in (("pt", agentray.PathTracer, agentray.PathTracerConfig),
+                               ("bdpt", agentray.BidirectionalPathTracer, agentray.BdptConfig)):
+        ref_img = np.empty(r * r * 3, np.float32)
+        cls(cfg_cls(spp=2048, max_depth=8, rr_depth=3, seed=99, film_precision=A.FILM_F64)).render(
+            scenes[k], cams[k], r, r, out=ref_img)
+        ref = ref_img.astype(np.float64)
+        job = cls(cfg_cls(spp=spp, max_depth=8, rr_depth=3, seed=123))
+        ids = [srv.submit(scenes[j["scene"]], cams[j["scene"]], make_integrator(agentray, j, 777 + i), j["res"],
+                          j["res"]) for i, j in enumerate(mix[:3])]
+        jid = srv.submit(scenes[k], cams[k], job, r, r)
+        ids += [srv.submit(scenes[j["scene"]], cams[j["scene"]], make_integrator(agentray, j, 888 + i), j["res"],
+                           j["res"]) for i, j in enumerate(mix[3:])]
+        for i in ids + [jid]:
+            wait_or_dump(srv, i)
+        served_img = srv.result(jid).reshape(-1).copy()
+        for i in ids + [jid]:
+            srv.forget(i)
+        plain_img = np.empty(r * r * 3, np.float32)
+        job.render(scenes[k], cams[k], r, r, out=plain_img)
+        out[name] = {"served_in_mix": rel(served_img, ref), "plain": rel(plain_img, ref)}
+    out["case"] = (f"served scene {k}, {r}x{r}, {spp} spp, depth 8; served inside a mix of {len(mix)} stream jobs; "
+                   f"reference: FP64-film 2048 spp")
+    return out
 
 
 def served_roofline(args, ctx, agentray, S, scenes, cams, built, peaks, peak_kind, torch):
@@ -520,6 +563,117 @@ def run_pt_cornell(args, rank, local, world, torch, ctx, barrier, dist, peaks, p
         print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ rooms ----
+def run_room(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind, stream):
+    """The 200k-triangle room: BDPT 512x512 x 64 spp, path length 10, FP64
+    film (bdpt_room), or GDPT 1024x1024 x 32 spp with the CG + FP64-refined
+    Poisson solve to relative residual 1e-6 (gdpt_room).  One step = one
+    full render."""
+    import agentray
+    import agentray.scenes as S
+    from agentray import _abi as A
+    from agentray.scene_data import integrator_cfg
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    sc, cam = S.room(4)
+    scene = agentray.Scene(ctx, sc)
+    ntri = scene.stats()["num_triangles"]
+    if args.workload == "bdpt_room":
+        W = H = 512
+        spp = 64
+        integ = agentray.BidirectionalPathTracer(agentray.BdptConfig(spp=spp, max_depth=10, rr_depth=3, seed=4 + rank,
+                                                                     film_precision=A.FILM_F64))
+        cfg = integrator_cfg(A.INTEGRATOR_BDPT, spp=1, max_depth=10, rr_depth=3)
+        desc = (f"bdpt_room: BDPT+MIS (power, beta 2) on the room ({ntri} tris: icospheres + 500 instanced boxes, "
+                f"Lambert/GGX 50/50, 2 quad lights), 512x512, 64 spp, max depth 10, FP64 film")
+        top = "bdpt_shadow"
+        dtype = "f32 transport, f64 film"
+    else:
+        W = H = 1024
+        spp = 32
+        integ = agentray.GradientDomainPathTracer(agentray.GdptConfig(
+            spp=spp, max_depth=8, rr_depth=3, alpha=0.2, poisson_solver=A.POISSON_CG, poisson_tolerance=1e-6,
+            seed=4 + rank))
+        cfg = integrator_cfg(A.INTEGRATOR_GDPT, spp=1, max_depth=8, rr_depth=3, alpha=0.2,
+                             poisson_solver=A.POISSON_SOR, poisson_iterations=200)
+        desc = (f"gdpt_room: GDPT (random replay, x/y shifts) on the room ({ntri} tris), 1024x1024, 32 spp, "
+                f"alpha 0.2, Poisson by FP32 CG with FP64 residual refinement to rel. residual 1e-6")
+        top = "pt_extend"
+        dtype = "f32 transport, f64 Poisson residuals"
+    out = torch.empty(W * H * 3, dtype=torch.float32, device="cuda")
+    for _ in range(max(3, args.warmup)):
+        integ.render(scene, cam, W, H, out=out)
+    torch.cuda.synchronize()
+    barrier()
+    evs = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            integ.render(scene, cam, W, H, out=out)
+            e1.record(stream)
+            evs.append((e0, e1))
+        torch.cuda.synchronize()
+    total_ms = sum(a.elapsed_time(b) for a, b in evs)
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    samples = W * H * spp
+    value = world * samples * args.steps / (total_ms / 1e3) / 1e6
+    stats = ctx.render_stats()
+    ctx.profile(True)
+    ctx.profile_reset()
+    flush.zero_()
+    integ.render(scene, cam, W, H, out=out)
+    torch.cuda.synchronize()
+    ctx.profile(False)
+    prof = ctx.profile_read()
+    pstats = ctx.render_stats()
+    host_out = np.empty(W * H * 3, np.float32)
+    e2e = []
+    for _ in range(max(1, min(3, args.steps))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        integ.render(scene, cam, W, H, out=host_out)
+        e2e.append(time.perf_counter() - t0)
+    e2e_value = samples / statistics.mean(e2e) / 1e6
+    if rank == 0:
+        nodes, tris = reference_traversal_counts(sc, cam)
+        b_ray = 32 + 16 + 32 * nodes + 36 * tris
+        ln, ms = prof.get(top, (1, 0.0))
+        rays = pstats["shadow_rays"] if top == "bdpt_shadow" else pstats["extend_rays"]
+        achieved = rays * b_ray / (ms / 1e3) / 1e9 if ms > 0 else 0.0
+        import oracle as O
+        osc = O.OracleScene(sc)
+        cores = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        osc.render(cam, cfg, W, H, sampler=O.SAMPLER_XOSHIRO, threads=cores)
+        cpu_s = time.perf_counter() - t0
+        osc.close()
+        line = {
+            "metric": METRIC, "value": value, "unit": "Mpath-samples/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded procedural scene)",
+            "config": {"workload": desc, "l2": "flushed (256 MiB write) before each timed step",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": e2e_value, "unit": "Mpath-samples/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": W * H * 3 * 4, "note": "scene resident; image returned to a host buffer"},
+            "gpu_launches": int(sum(v[0] for v in prof.values()) * args.steps),
+            "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peaks["hbm_gbs"],
+                         "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                         "peak_kind": peak_kind,
+                         "bytes_model": f"{rays} rays x (48 + 32*{nodes:.2f} nodes + 36*{tris:.2f} tris) B over "
+                                        f"{ln} launches; reference-traversal counts of primary/interior rays"},
+            "kernels_ms": {k: {"launches": v[0], "ms": v[1]} for k, v in prof.items()},
+            "render_stats": stats, "clocks": clk.summary(),
+            "cpu_baseline": {"value": W * H / cpu_s / 1e6, "unit": "Mpath-samples/s", "cores": cores, "kind": "port",
+                             "sample": f"one {W}x{H} render at 1 spp, reference sampler"}}
+        print(json.dumps(line), flush=True)
+
+
 # -------------------------------------------------------------------- bvh ----
 def run_bvh(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind, stream):
     import agentray
@@ -612,7 +766,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="served", choices=["served", "pt_cornell", "pt_served4", "bvh"])
+    ap.add_argument("--workload", default="served",
+                    choices=["served", "pt_cornell", "pt_served4", "bdpt_room", "gdpt_room", "bvh"])
     ap.add_argument("--jobs", type=int, default=2000)
     ap.add_argument("--window-jobs", dest="window_jobs", type=int, default=16)
     ap.add_argument("--served-jobs", dest="served_jobs", type=int, default=160)
@@ -647,6 +802,8 @@ def main():
         run_served(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind)
     elif args.workload in ("pt_cornell", "pt_served4"):
         run_pt_cornell(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind, stream)
+    elif args.workload in ("bdpt_room", "gdpt_room"):
+        run_room(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind, stream)
     else:
         run_bvh(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind, stream)
     if dist is not None:

@@ -1,0 +1,103 @@
+"""relMSE against an FP64 high-spp converged oracle.
+
+The converged reference is the oracle (the C++ restatement of the reference's
+integrators) instantiated in FP64 -- geometry, traversal, shading and film all
+in double -- at high spp.  Each image is scored by
+
+    relMSE = mean over pixels and channels of (x - ref)^2 / (ref^2 + 1e-2).
+
+The GPU (FP32 transport) must reach the same relMSE as the FP32 oracle at the
+same spp: on the same sample streams the two relMSEs agree to 2% (the images
+agree pixel by pixel), and on independent seeds the ratio of replicate means
+stays within [0.6, 1.65] -- relMSE is heavy-tailed (a single 16-spp BDPT
+replicate ranges over 3x), so this second bar is loose.  Equal relMSE at equal
+spp is the bar under which batched and plain GPU throughput are compared.  The
+measured values print with `pytest -s`.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import agentray
+import agentray.scenes as S
+import oracle as O
+from agentray import _abi as A
+from agentray.scene_data import integrator_cfg
+
+pytestmark = pytest.mark.gpu
+
+
+def relmse(x, ref):
+    return float(np.mean((x - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+
+def _render_gpu(ctx, scene, cam, cfg, w, h):
+    out = np.empty(w * h * 3, np.float32)
+    agentray.check(agentray.lib().ar_render(ctx.handle, scene.handle, C.byref(cam.desc()), C.byref(cfg), w, h,
+                                            out.ctypes.data, 0))
+    return out.reshape(h, w, 3).astype(np.float64)
+
+
+def _compare(ctx, sc, cam, kind, ref_cfg, w, h, spp, reps=8, **kw):
+    """Mean relMSE of GPU and FP32-oracle replicates: GPU seeds 1000+k, oracle
+    seeds 1000+k (same streams) and 2000+k (independent)."""
+    ref = O.OracleScene(sc, precision=64).render(cam, ref_cfg, w, h, sampler=O.SAMPLER_COUNTER)
+    g = agentray.Scene(ctx, sc)
+    osc = O.OracleScene(sc)
+    gpu = [relmse(_render_gpu(ctx, g, cam, integrator_cfg(kind, spp=spp, seed=1000 + k, **kw), w, h), ref)
+           for k in range(reps)]
+    same = [relmse(osc.render(cam, integrator_cfg(kind, spp=spp, seed=1000 + k, **kw), w, h,
+                              sampler=O.SAMPLER_COUNTER), ref) for k in range(reps)]
+    indep = [relmse(osc.render(cam, integrator_cfg(kind, spp=spp, seed=2000 + k, **kw), w, h,
+                               sampler=O.SAMPLER_COUNTER), ref) for k in range(reps)]
+    return float(np.mean(gpu)), float(np.mean(same)), float(np.mean(indep)), ref, g
+
+
+def _check(gpu, same, indep):
+    assert abs(gpu / same - 1.0) <= 0.02, (gpu, same)
+    assert 0.6 <= gpu / indep <= 1.65, (gpu, indep)
+
+
+def test_pt_relmse_equals_oracle(ctx):
+    sc, cam = S.cornell_box(1)
+    w = h = 48
+    ref_cfg = integrator_cfg(A.INTEGRATOR_PT, spp=4096, max_depth=8, rr_depth=3, seed=7)
+    gpu, same, indep, ref, g = _compare(ctx, sc, cam, A.INTEGRATOR_PT, ref_cfg, w, h, spp=16, max_depth=8,
+                                        rr_depth=3)
+    print(f"\nPT Cornell {w}x{h} 16 spp: relMSE GPU {gpu:.5f}  FP32 oracle same seeds {same:.5f}, "
+          f"independent {indep:.5f}  (ref: FP64 oracle 4096 spp)")
+    _check(gpu, same, indep)
+    # high spp: the FP64-film GPU image converges on the FP64 oracle
+    hi = relmse(_render_gpu(ctx, g, cam, integrator_cfg(A.INTEGRATOR_PT, spp=1024, seed=3,
+                                                        film_precision=A.FILM_F64), w, h), ref)
+    print(f"PT Cornell {w}x{h} 1024 spp, FP64 film: relMSE {hi:.6f}")
+    assert hi < gpu / 32
+
+
+def test_bdpt_relmse_equals_oracle(ctx):
+    sc, cam = S.cornell_box(1)
+    w = h = 32
+    ref_cfg = integrator_cfg(A.INTEGRATOR_BDPT, spp=2048, max_depth=6, rr_depth=3, seed=7)
+    gpu, same, indep, _, _ = _compare(ctx, sc, cam, A.INTEGRATOR_BDPT, ref_cfg, w, h, spp=16, max_depth=6,
+                                      rr_depth=3)
+    print(f"\nBDPT Cornell {w}x{h} 16 spp: relMSE GPU {gpu:.5f}  FP32 oracle same seeds {same:.5f}, "
+          f"independent {indep:.5f}  (ref: FP64 oracle 2048 spp)")
+    _check(gpu, same, indep)
+
+
+def test_gdpt_relmse_equals_oracle(ctx):
+    sc, cam = S.cornell_box(1)
+    w, h = 48, 40
+    # GDPT's reconstruction converges to the PT image: the reference is FP64 PT.
+    ref_cfg = integrator_cfg(A.INTEGRATOR_PT, spp=4096, max_depth=6, rr_depth=3, seed=7)
+    gpu, same, indep, ref, g = _compare(ctx, sc, cam, A.INTEGRATOR_GDPT, ref_cfg, w, h, spp=16, max_depth=6,
+                                        rr_depth=3)
+    print(f"\nGDPT (SOR) Cornell {w}x{h} 16 spp: relMSE GPU {gpu:.5f}  FP32 oracle same seeds {same:.5f}, "
+          f"independent {indep:.5f}  (ref: FP64 oracle PT 4096 spp)")
+    _check(gpu, same, indep)
+    cg = np.mean([relmse(_render_gpu(ctx, g, cam, integrator_cfg(
+        A.INTEGRATOR_GDPT, spp=16, max_depth=6, rr_depth=3, seed=1000 + k, poisson_solver=A.POISSON_CG,
+        poisson_tolerance=1e-6), w, h), ref) for k in range(8)])
+    print(f"GDPT (CG + FP64 refinement, 1e-6) Cornell {w}x{h} 16 spp: relMSE GPU {cg:.5f}")
+    assert 0.6 <= cg / gpu <= 1.65, (cg, gpu)

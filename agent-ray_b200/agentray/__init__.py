@@ -32,6 +32,7 @@ class Context:
     """One CUDA device + stream (ar_context)."""
 
     def __init__(self, device=0):
+        self.device = device
         self.handle = C.c_void_p()
         check(lib().ar_context_create(device, C.byref(self.handle)))
 
@@ -63,6 +64,23 @@ class Context:
         keys = names.value.decode().split("\n")[: n.value]
         return {k: (int(ln[i]), float(ms[i])) for i, k in enumerate(keys)}
 
+    def tuning(self):
+        """Launch shapes and queue capacities of this context (ar_tuning)."""
+        t = A.Tuning()
+        check(lib().ar_context_get_tuning(self.handle, C.byref(t)))
+        return {k: getattr(t, k) for k, _ in A.Tuning._fields_}
+
+    def set_tuning(self, **kw):
+        """Updates some of path_capacity, traversal_blocks_per_sm, shade_block,
+        bdpt_batch_mib (the rest keep their values)."""
+        cur = self.tuning()
+        unknown = set(kw) - set(cur)
+        if unknown:
+            raise ValueError(f"unknown tuning keys {sorted(unknown)}")
+        cur.update(kw)
+        t = A.Tuning(**cur)
+        check(lib().ar_context_set_tuning(self.handle, C.byref(t)))
+
     def close(self):
         if self.handle:
             lib().ar_context_destroy(self.handle)
@@ -91,8 +109,8 @@ class Scene:
         check(lib().ar_scene_get_stats(self.handle, C.byref(s)))
         return {k: getattr(s, k) for k, _ in A.SceneStats._fields_ if not k.startswith("_")}
 
-    def rebuild(self, max_leaf_size=3, sah_bins=32, build_threads=0):
-        o = A.AccelOpts(max_leaf_size, sah_bins, build_threads, 0)
+    def rebuild(self, max_leaf_size=3, sah_bins=32, build_threads=0, bvh_width=8):
+        o = A.AccelOpts(max_leaf_size, sah_bins, build_threads, bvh_width)
         check(lib().ar_scene_build_accel(self.ctx.handle, self.handle, C.byref(o)))
 
     @staticmethod
@@ -197,6 +215,9 @@ class GdptConfig:
     poisson_tolerance: float = 1e-6
     seed: int = 0
     film_precision: int = A.FILM_F32
+    # extension: A.GDPT_CONSISTENT_DIVERGENCE solves with -div G (converges to
+    # the primal-domain image); 0 reproduces the reference's +div G
+    gdpt_flags: int = 0
 
 
 class _Integrator:
@@ -213,7 +234,7 @@ class _Integrator:
                               sor_omega=getattr(c, "sor_omega", 1.6),
                               poisson_solver=getattr(c, "poisson_solver", A.POISSON_SOR),
                               poisson_tolerance=getattr(c, "poisson_tolerance", 1e-6), seed=c.seed,
-                              film_precision=c.film_precision)
+                              film_precision=c.film_precision, gdpt_flags=getattr(c, "gdpt_flags", 0))
 
     def render(self, scene: Scene, camera: Camera, width: int, height: int, out=None) -> Film:
         """Integrator::render.  `out` may be a CUDA float32 tensor of W*H*3 to
@@ -327,7 +348,7 @@ class Server:
 
 
 def poisson_reconstruct(ctx: Context, primal, grad_x, grad_y, alpha=0.2, solver=A.POISSON_SOR, iterations=200,
-                        omega=1.6, tolerance=1e-6):
+                        omega=1.6, tolerance=1e-6, gdpt_flags=0):
     """screened_poisson_reconstruct on the GPU for (H, W, 3) float32 films.
     Returns (image, fp64 relative residual or -1 for SOR)."""
     h, w, _ = primal.shape
@@ -336,7 +357,7 @@ def poisson_reconstruct(ctx: Context, primal, grad_x, grad_y, alpha=0.2, solver=
     y = np.ascontiguousarray(grad_y, np.float32)
     out = np.empty_like(p)
     cfg = integrator_cfg(A.INTEGRATOR_GDPT, alpha=alpha, poisson_iterations=iterations, sor_omega=omega,
-                         poisson_solver=solver, poisson_tolerance=tolerance)
+                         poisson_solver=solver, poisson_tolerance=tolerance, gdpt_flags=gdpt_flags)
     res = C.c_double(0.0)
     check(lib().ar_poisson_reconstruct(ctx.handle, C.byref(cfg), w, h, p.ctypes.data, x.ctypes.data, y.ctypes.data,
                                        out.ctypes.data, 0, C.byref(res)))

@@ -31,6 +31,7 @@ POISSON_SOR = 0
 POISSON_CG = 1
 FILM_F32 = 0
 FILM_F64 = 1
+GDPT_CONSISTENT_DIVERGENCE = 1
 
 u32 = C.c_uint32
 f32 = C.c_float
@@ -72,7 +73,7 @@ class IntegratorCfg(C.Structure):
     _fields_ = [("integrator", u32), ("spp", u32), ("max_depth", u32), ("rr_depth", u32), ("mis_mode", u32),
                 ("mis_beta", f32), ("alpha", f32), ("poisson_iterations", u32), ("sor_omega", f32),
                 ("poisson_solver", u32), ("poisson_tolerance", C.c_double), ("seed", C.c_uint64),
-                ("film_precision", u32), ("_pad", u32)]
+                ("film_precision", u32), ("gdpt_flags", u32)]
 
 
 class RayBatch(C.Structure):
@@ -85,7 +86,22 @@ class Hit(C.Structure):
 
 
 class AccelOpts(C.Structure):
-    _fields_ = [("max_leaf_size", u32), ("sah_bins", u32), ("build_threads", u32), ("_pad", u32)]
+    _fields_ = [("max_leaf_size", u32), ("sah_bins", u32), ("build_threads", u32), ("bvh_width", u32)]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("path_capacity", u32), ("traversal_blocks_per_sm", u32), ("shade_block", u32),
+                ("bdpt_batch_mib", u32)]
+
+
+class TuneOpts(C.Structure):
+    _fields_ = [("integrator", u32), ("width", u32), ("height", u32), ("spp", u32), ("max_depth", u32),
+                ("repeats", u32), ("tune_accel", u32), ("_pad", u32)]
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("tuning", Tuning), ("accel", AccelOpts), ("default_ms", C.c_double), ("best_ms", C.c_double),
+                ("candidates", u32), ("_pad", u32)]
 
 
 class SceneStats(C.Structure):

@@ -22,6 +22,10 @@ SIGNATURES = {
     "ar_scene_create": (C.c_int, [C.c_void_p, C.POINTER(A.SceneDesc), C.POINTER(C.c_void_p)]),
     "ar_scene_destroy": (C.c_int, [C.c_void_p]),
     "ar_scene_build_accel": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(A.AccelOpts)]),
+    "ar_context_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(A.Tuning)]),
+    "ar_context_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(A.Tuning)]),
+    "ar_autotune": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(A.CameraDesc), C.POINTER(A.TuneOpts),
+                              C.POINTER(A.TuneResult)]),
     "ar_scene_get_stats": (C.c_int, [C.c_void_p, C.POINTER(A.SceneStats)]),
     "ar_trace_closest": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(A.RayBatch), C.c_void_p, C.c_void_p,
                                    C.c_uint32]),

@@ -165,7 +165,7 @@ class SceneData:
 
 def integrator_cfg(integrator=A.INTEGRATOR_PT, spp=16, max_depth=8, rr_depth=3, mis_mode=A.MIS_POWER,
                    mis_beta=2.0, alpha=0.2, poisson_iterations=200, sor_omega=1.6, poisson_solver=A.POISSON_SOR,
-                   poisson_tolerance=1e-6, seed=0, film_precision=A.FILM_F32):
+                   poisson_tolerance=1e-6, seed=0, film_precision=A.FILM_F32, gdpt_flags=0):
     c = A.IntegratorCfg()
     c.integrator = integrator
     c.spp = spp
@@ -180,4 +180,5 @@ def integrator_cfg(integrator=A.INTEGRATOR_PT, spp=16, max_depth=8, rr_depth=3, 
     c.poisson_tolerance = poisson_tolerance
     c.seed = seed
     c.film_precision = film_precision
+    c.gdpt_flags = gdpt_flags
     return c

@@ -134,6 +134,10 @@ struct ar_context {
     bool stats_pending = false;
     ar::PathEngine* engine = nullptr;  // streaming wavefront engine for ar_render
     uint32_t engine_capacity = 1u << 21;
+    // launch shapes (ar_tuning)
+    uint32_t trav_blocks_per_sm = 8;       // persistent traversal grid, blocks per SM
+    uint32_t shade_block = 256;            // threads per block of the shading stage
+    size_t bdpt_budget = size_t(3) << 30;  // HBM for one plain-path BDPT batch
     ar::BdptBatcher* bdpt = nullptr;   // BDPT batch buffers for ar_render
 };
 
@@ -155,6 +159,7 @@ struct ar_scene {
         light_cdf, light_pmf;
     ar::DevScene view{};
     ar_scene_stats stats{};
+    ar_accel_opts accel{};  // options of the last build
     std::vector<ar::LightRecord> lights_h;
     std::vector<ar::MaterialRecord> materials_h;
     uint32_t light_dist = 0;

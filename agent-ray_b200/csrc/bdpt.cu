@@ -817,7 +817,7 @@ void bdpt_run_batch(BdptBatcher* b, const std::vector<BdJob>& jobs, const std::v
     for (uint32_t d = 0; d < max_depth; ++d) {
         {
             KernelScope ks(ctx->prof, ctx->stream, "bdpt_extend");
-            k_bd_extend<<<ctx->num_sms * kTraversalBlocksPerSm, 128, 0, ctx->stream>>>(P, d, err);
+            k_bd_extend<<<ctx->num_sms * int(ctx->trav_blocks_per_sm), 128, 0, ctx->stream>>>(P, d, err);
         }
         {
             KernelScope ks(ctx->prof, ctx->stream, "bdpt_vertex");
@@ -838,7 +838,7 @@ void bdpt_run_batch(BdptBatcher* b, const std::vector<BdJob>& jobs, const std::v
     }
     {
         KernelScope ks(ctx->prof, ctx->stream, "bdpt_shadow");
-        k_bd_shadow<<<ctx->num_sms * kTraversalBlocksPerSm, 128, 0, ctx->stream>>>(P, err);
+        k_bd_shadow<<<ctx->num_sms * int(ctx->trav_blocks_per_sm), 128, 0, ctx->stream>>>(P, err);
     }
     k_bd_count<<<1, 32, 0, ctx->stream>>>(P.counts, max_depth, ctx->stats_d.as<unsigned long long>(), err);
     AR_CUDA(cudaGetLastError());
@@ -868,7 +868,7 @@ void render_bdpt_film(ar_context* ctx, const ar_scene* sc, const CameraDev& cam,
                       uint32_t w, uint32_t h, void* film) {
     AR_REQUIRE(cfg.max_depth <= 62, AR_ERR_INVALID_ARGUMENT, "max_depth must be <= 62");
     const uint64_t total = uint64_t(w) * h * cfg.spp;
-    const size_t budget = size_t(3) << 30;
+    const size_t budget = ctx->bdpt_budget;
     const size_t per = bdpt_batch_bytes(cfg.max_depth, 1024) / 1024 + 1;
     const uint32_t batch = uint32_t(std::max<uint64_t>(1024, std::min<uint64_t>(total, budget / per)));
     if (!ctx->bdpt || bdpt_max_depth_cap(ctx->bdpt) < cfg.max_depth || bdpt_batch_capacity(ctx->bdpt) < batch) {

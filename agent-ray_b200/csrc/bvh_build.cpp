@@ -249,6 +249,7 @@ WideBuild build_wide_bvh(const std::vector<PrimBox>& boxes, const BuildOptions& 
     if (boxes.empty()) return out;
     BuildOptions opts = opts_in;
     opts.max_leaf = std::max(1u, std::min(3u, opts.max_leaf));
+    opts.width = std::max(2u, std::min(8u, opts.width));
     std::vector<BinNode> bn;
     std::vector<uint32_t> order;
     build_binary(boxes, opts, bn, order);
@@ -261,14 +262,14 @@ WideBuild build_wide_bvh(const std::vector<PrimBox>& boxes, const BuildOptions& 
         Item it = queue.front();
         queue.pop_front();
         out.depth = std::max(out.depth, it.depth);
-        // Gather up to 8 children by opening the largest internal child.
+        // Gather up to `width` (<= 8) children by opening the largest internal child.
         std::vector<uint32_t> ch;
         if (bn[it.bin].count > 0) {
             ch.push_back(it.bin);
         } else {
             ch.push_back(bn[it.bin].left);
             ch.push_back(bn[it.bin].right);
-            while (ch.size() < 8) {
+            while (ch.size() < opts.width) {
                 int best = -1;
                 float best_a = -1.f;
                 for (size_t i = 0; i < ch.size(); ++i) {

@@ -28,7 +28,10 @@ void check_device_flag(ar_context* ctx) {
         AR_CUDA(cudaMemsetAsync(ctx->err_flag.ptr, 0, sizeof(int), ctx->stream));
         AR_CUDA(cudaStreamSynchronize(ctx->stream));
         throw ArError{flag == 2 ? AR_ERR_TIMEOUT : AR_ERR_INTERNAL,
-                      flag == 1 ? "traversal stack overflow" : "device work budget exceeded"};
+                      flag == 1   ? "traversal stack overflow"
+                      : flag == 3 ? "traversal step budget exceeded"
+                      : flag == 4 ? "BDPT connection queue overflow"
+                                  : "device work budget exceeded"};
     }
 }
 

@@ -3,6 +3,7 @@
 //
 // System per colour channel (5-point stencil, Neumann borders):
 //   (alpha + N(x)) I(x) - sum_{n in N(x)} I(n) = alpha * primal(x) + div G(x)
+// (the reference's sign; AR_GDPT_CONSISTENT_DIVERGENCE subtracts div G instead)
 //
 // Two solvers:
 //   * red-black SOR, the reference method: each half sweep updates one colour
@@ -24,7 +25,8 @@ namespace ar {
 namespace {
 
 __global__ void k_rhs(uint32_t w, uint32_t h, const float* __restrict__ primal, const float* __restrict__ gx,
-                      const float* __restrict__ gy, float alpha, float* __restrict__ rhs, float* __restrict__ img) {
+                      const float* __restrict__ gy, float alpha, bool neg_div, float* __restrict__ rhs,
+                      float* __restrict__ img) {
     const uint32_t n = w * h;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t x = i % w, y = i / w;
@@ -33,7 +35,8 @@ __global__ void k_rhs(uint32_t w, uint32_t h, const float* __restrict__ primal, 
             if (x > 0) div -= gx[3 * (i - 1) + c];
             div += gy[3 * i + c];
             if (y > 0) div -= gy[3 * (i - w) + c];
-            rhs[3 * i + c] = alpha * primal[3 * i + c] + div;
+            const float a = alpha * primal[3 * i + c];
+            rhs[3 * i + c] = neg_div ? a - div : a + div;
             img[3 * i + c] = primal[3 * i + c];
         }
     }
@@ -110,7 +113,7 @@ __device__ __forceinline__ void block_add3(double a0, double a1, double a2, doub
 
 // b (f64) = alpha*primal + div G; x (f64) = primal; bb += |b|^2.
 __global__ void k_cg_setup(uint32_t w, uint32_t h, const float* primal, const float* gx, const float* gy, double alpha,
-                           double* b, double* x, double* bb) {
+                           bool neg_div, double* b, double* x, double* bb) {
     const uint32_t n = w * h;
     double a[3] = {0, 0, 0};
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -120,7 +123,8 @@ __global__ void k_cg_setup(uint32_t w, uint32_t h, const float* primal, const fl
             if (xx > 0) div -= gx[3 * (i - 1) + c];
             div += gy[3 * i + c];
             if (yy > 0) div -= gy[3 * (i - w) + c];
-            const double bv = alpha * double(primal[3 * i + c]) + div;
+            const double av = alpha * double(primal[3 * i + c]);
+            const double bv = neg_div ? av - div : av + div;
             b[3 * i + c] = bv;
             x[3 * i + c] = primal[3 * i + c];
             a[c] += bv * bv;
@@ -215,7 +219,8 @@ void poisson_sor_with_scratch(cudaStream_t stream, int num_sms, const ar_integra
                               float* out) {
     const size_t n = size_t(w) * h;
     const int grid = std::max(1, std::min(int((n + 255) / 256), num_sms * 8));
-    k_rhs<<<grid, 256, 0, stream>>>(w, h, primal, gx, gy, cfg.alpha, rhs, img);
+    k_rhs<<<grid, 256, 0, stream>>>(w, h, primal, gx, gy, cfg.alpha,
+                                     (cfg.gdpt_flags & AR_GDPT_CONSISTENT_DIVERGENCE) != 0, rhs, img);
     for (uint32_t it = 0; it < cfg.poisson_iterations; ++it)
         for (uint32_t parity = 0; parity < 2; ++parity)
             k_sor_half<<<grid, 256, 0, stream>>>(w, h, parity, rhs, img, cfg.alpha, cfg.sor_omega);
@@ -232,7 +237,8 @@ void poisson_reconstruct(ar_context* ctx, const ar_integrator_cfg& cfg, uint32_t
         ctx->solver.ensure(2 * 3 * n * sizeof(float));
         float* rhs = ctx->solver.buf.as<float>();
         float* img = rhs + 3 * n;
-        k_rhs<<<grid, 256, 0, st>>>(w, h, primal, gx, gy, cfg.alpha, rhs, img);
+        k_rhs<<<grid, 256, 0, st>>>(w, h, primal, gx, gy, cfg.alpha,
+                                     (cfg.gdpt_flags & AR_GDPT_CONSISTENT_DIVERGENCE) != 0, rhs, img);
         for (uint32_t it = 0; it < cfg.poisson_iterations; ++it)
             for (uint32_t parity = 0; parity < 2; ++parity)
                 k_sor_half<<<grid, 256, 0, st>>>(w, h, parity, rhs, img, cfg.alpha, cfg.sor_omega);
@@ -257,7 +263,8 @@ void poisson_reconstruct(ar_context* ctx, const ar_integrator_cfg& cfg, uint32_t
     scal = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(scal) + 63) & ~uintptr_t(63));
     double* bb = scal + 9;
     AR_CUDA(cudaMemsetAsync(scal, 0, 16 * sizeof(double), st));
-    k_cg_setup<<<grid, 256, 0, st>>>(w, h, primal, gx, gy, alpha, b, x, bb);
+    k_cg_setup<<<grid, 256, 0, st>>>(w, h, primal, gx, gy, alpha,
+                                     (cfg.gdpt_flags & AR_GDPT_CONSISTENT_DIVERGENCE) != 0, b, x, bb);
     double hb[16];
     double res = 0.0;
     uint32_t total = 0;

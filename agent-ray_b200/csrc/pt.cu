@@ -376,13 +376,17 @@ struct PathEngine {
     } stage[2];
     int stage_next = 0;
 
+    // The five stages of one tick, with the context's launch shapes (each
+    // stage bracketed by a profiler scope when profiling is on).
     void launch_tick(int q, cudaStream_t s) {
         const int wide = ctx->num_sms * 8;
-        k_plan<<<1, 32, 0, s>>>(E, q);
-        k_generate<<<wide, 256, 0, s>>>(E, q);
-        k_extend<<<ctx->num_sms * kTraversalBlocksPerSm, 128, 0, s>>>(E, q);
-        k_shade<<<wide, 256, 0, s>>>(E, q);
-        k_shadow<<<ctx->num_sms * kTraversalBlocksPerSm, 128, 0, s>>>(E, q);
+        const int tgrid = ctx->num_sms * int(ctx->trav_blocks_per_sm);
+        const int sb = int(ctx->shade_block);
+        { KernelScope k(ctx->prof, s, "pt_plan"); k_plan<<<1, 32, 0, s>>>(E, q); }
+        { KernelScope k(ctx->prof, s, "pt_generate"); k_generate<<<wide, 256, 0, s>>>(E, q); }
+        { KernelScope k(ctx->prof, s, "pt_extend"); k_extend<<<tgrid, 128, 0, s>>>(E, q); }
+        { KernelScope k(ctx->prof, s, "pt_shade"); k_shade<<<wide * (256 / sb), sb, 0, s>>>(E, q); }
+        { KernelScope k(ctx->prof, s, "pt_shadow"); k_shadow<<<tgrid, 128, 0, s>>>(E, q); }
     }
 
     void build_graphs() {
@@ -502,13 +506,7 @@ void engine_tick(PathEngine* e) {
     const int q = e->parity;
     if (ctx->prof.on) {
         // Profiling: launch the stages individually, each bracketed by events.
-        cudaStream_t s = ctx->stream;
-        const int wide = ctx->num_sms * 8;
-        { KernelScope k(ctx->prof, s, "pt_plan"); k_plan<<<1, 32, 0, s>>>(e->E, q); }
-        { KernelScope k(ctx->prof, s, "pt_generate"); k_generate<<<wide, 256, 0, s>>>(e->E, q); }
-        { KernelScope k(ctx->prof, s, "pt_extend"); k_extend<<<ctx->num_sms * kTraversalBlocksPerSm, 128, 0, s>>>(e->E, q); }
-        { KernelScope k(ctx->prof, s, "pt_shade"); k_shade<<<wide, 256, 0, s>>>(e->E, q); }
-        { KernelScope k(ctx->prof, s, "pt_shadow"); k_shadow<<<ctx->num_sms * kTraversalBlocksPerSm, 128, 0, s>>>(e->E, q); }
+        e->launch_tick(q, ctx->stream);
         AR_CUDA(cudaGetLastError());
     } else {
         if (e->captured_stream != ctx->stream) e->build_graphs();

@@ -90,10 +90,12 @@ void invert4x4(const float* m, float* out) {
 
 void build_scene_accel(ar_scene* s, const ar_accel_opts* o) {
     auto t0 = std::chrono::steady_clock::now();
+    s->accel = o ? *o : ar_accel_opts{};
     BuildOptions bo;
     if (o) {
         if (o->max_leaf_size) bo.max_leaf = o->max_leaf_size;
         if (o->sah_bins) bo.bins = o->sah_bins;
+        if (o->bvh_width) bo.width = o->bvh_width;
         bo.threads = o->build_threads;
     }
     std::vector<WideNode> nodes;

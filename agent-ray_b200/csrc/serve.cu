@@ -443,6 +443,10 @@ int ar_server_create(ar_context* ctx, const ar_server_opts* o, ar_server** out) 
         S.t0 = std::chrono::steady_clock::now();
         S.ctx_pt = context_create_internal(ctx->device);
         S.ctx_bd = context_create_internal(ctx->device);
+        for (ar_context* c : {S.ctx_pt, S.ctx_bd}) {  // launch shapes follow the caller's context
+            c->trav_blocks_per_sm = ctx->trav_blocks_per_sm;
+            c->shade_block = ctx->shade_block;
+        }
         S.engine = engine_create(S.ctx_pt, S.opts.path_capacity);
         S.bdpt = bdpt_create(S.ctx_bd, S.opts.bdpt_max_depth, S.opts.bdpt_batch_samples);
         for (uint32_t i = S.opts.max_active_jobs; i-- > 0;) S.free_slots.push_back(i);

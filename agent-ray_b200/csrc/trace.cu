@@ -42,7 +42,7 @@ void launch_trace(ar_context* ctx, const ar_scene* sc, const float4* ot, const f
     // Persistent grid; lanes fetch rays from a cursor.  Batches above 2^31 rays go in slices.
     const uint64_t kSlice = 1ull << 31;
     const int grid = std::max<int>(1, int(std::min<uint64_t>((n + 127) / 128,
-                                                              uint64_t(ctx->num_sms) * kTraversalBlocksPerSm)));
+                                                              uint64_t(ctx->num_sms) * ctx->trav_blocks_per_sm)));
     uint32_t* cursor = ctx->fetch.as<uint32_t>();
     KernelScope ks(ctx->prof, ctx->stream, any ? "trace_any" : "trace_closest");
     for (uint64_t off = 0; off < n; off += kSlice) {

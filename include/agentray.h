@@ -155,6 +155,15 @@ enum ar_poisson_solver {
 };
 enum ar_film_precision { AR_FILM_F32 = 0, AR_FILM_F64 = 1 };
 
+/* GDPT options beyond the reference (extension; off by default).
+ * AR_GDPT_CONSISTENT_DIVERGENCE: the reference builds the Poisson right-hand
+ * side as alpha*primal + div G (gradient_domain_pt.rs:503-541) while its
+ * stencil is (alpha + N) I - sum I(n); with G = I(x+1) - I(x) the consistent
+ * right-hand side is alpha*primal - div G.  With the flag set the solve uses
+ * that sign and converges to the primal-domain image; without it the output
+ * equals the reference's. */
+enum ar_gdpt_flags { AR_GDPT_CONSISTENT_DIVERGENCE = 1 };
+
 typedef struct ar_integrator_cfg {
     uint32_t integrator;             /* ar_integrator_kind */
     uint32_t spp;
@@ -169,7 +178,7 @@ typedef struct ar_integrator_cfg {
     double poisson_tolerance;        /* CG: relative residual target (FP64) */
     uint64_t seed;                   /* sampler key; 0 reproduces the default stream */
     uint32_t film_precision;         /* ar_film_precision */
-    uint32_t _pad;
+    uint32_t gdpt_flags;             /* ar_gdpt_flags; 0 reproduces the reference */
 } ar_integrator_cfg;
 
 /* ---- ray batches (src/geometry.rs:3-20, src/accel/bvh.rs:10-20) ---- */
@@ -195,7 +204,7 @@ typedef struct ar_accel_opts {
     uint32_t max_leaf_size;          /* 1..3 triangles per wide-BVH leaf (default 3) */
     uint32_t sah_bins;               /* binned SAH bins (default 32) */
     uint32_t build_threads;          /* host threads for the build (0 = all cores) */
-    uint32_t _pad;
+    uint32_t bvh_width;              /* children per node, 2..8 (0 = 8); the node format is 8-wide */
 } ar_accel_opts;
 
 typedef struct ar_scene_stats {
@@ -220,6 +229,45 @@ int ar_context_destroy(ar_context* ctx);
  * context's own; NULL restores the context stream. */
 int ar_context_set_stream(ar_context* ctx, void* cuda_stream);
 int ar_context_synchronize(ar_context* ctx);
+
+/* Launch and queue parameters of a context (the autotuner's search space).
+ * No reference counterpart: the reference's CPU integrators have no such knobs. */
+typedef struct ar_tuning {
+    uint32_t path_capacity;          /* PT/GDPT engine path slots (queue capacity; 0: 2^21) */
+    uint32_t traversal_blocks_per_sm;/* persistent traversal grid, 128-thread blocks per SM, 1..8 (0: 8) */
+    uint32_t shade_block;            /* threads per block of the shading stage: 64, 128 or 256 (0: 256) */
+    uint32_t bdpt_batch_mib;         /* HBM for one BDPT batch of ar_render, MiB (0: 3072) */
+} ar_tuning;
+
+int ar_context_get_tuning(const ar_context* ctx, ar_tuning* out);
+/* Applies `t` to later renders (synchronises the context's stream first). */
+int ar_context_set_tuning(ar_context* ctx, const ar_tuning* t);
+
+typedef struct ar_tune_opts {
+    uint32_t integrator;             /* AR_INTEGRATOR_PT / _BDPT / _GDPT: the workload timed */
+    uint32_t width, height;          /* size of the timed render (0: 256 x 256) */
+    uint32_t spp;                    /* spp of the timed render (0: 4) */
+    uint32_t max_depth;              /* 0: 8 */
+    uint32_t repeats;                /* timed renders per candidate, the median counts (0: 3) */
+    uint32_t tune_accel;             /* 1: also search BVH width and leaf size (rebuilds the scene's accel) */
+    uint32_t _pad;
+} ar_tune_opts;
+
+typedef struct ar_tune_result {
+    ar_tuning tuning;                /* best launch/queue parameters (applied to ctx) */
+    ar_accel_opts accel;             /* best build options (the scene is left built with them) */
+    double default_ms;               /* median render time with the starting parameters */
+    double best_ms;                  /* median render time with the result */
+    uint32_t candidates;             /* configurations timed */
+    uint32_t _pad;
+} ar_tune_result;
+
+/* Project autotuner: coordinate descent over BVH width, leaf size, traversal
+ * grid, shading block size and queue capacities, each candidate timed with
+ * CUDA events on the context's stream.  Leaves the best tuning applied to `ctx`
+ * and `scene` built with the best accel options.  No reference counterpart. */
+int ar_autotune(ar_context* ctx, ar_scene* scene, const ar_camera_desc* camera, const ar_tune_opts* opts,
+                ar_tune_result* out);
 
 int ar_scene_create(ar_context* ctx, const ar_scene_desc* desc, ar_scene** out);
 int ar_scene_destroy(ar_scene* scene);

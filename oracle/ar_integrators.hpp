@@ -595,9 +595,11 @@ void render_gdpt_films(const Scene<T>& sc, const Camera<T>& cam, const ar_integr
 
 // screened_poisson_reconstruct (:449-630): RHS = alpha*primal + div G, then
 // red-black SOR; result clamped at 0.  Buffers are interleaved RGB (W*H*3).
+// neg_div (an extension, off for the reference): RHS = alpha*primal - div G,
+// the sign consistent with the stencil for G = I(x+1) - I(x).
 template <class T>
 void poisson_sor(uint32_t w, uint32_t h, const T* primal, const T* gx, const T* gy, T alpha, uint32_t iters, T omega,
-                 T* out) {
+                 T* out, bool neg_div = false) {
     size_t n = size_t(w) * h;
     std::vector<T> img(3 * n), rhs(3 * n);
     for (size_t i = 0; i < 3 * n; ++i) img[i] = primal[i];
@@ -609,7 +611,8 @@ void poisson_sor(uint32_t w, uint32_t h, const T* primal, const T* gx, const T* 
                 if (x > 0) div -= gx[3 * (idx - 1) + c];
                 div += gy[3 * idx + c];
                 if (y > 0) div -= gy[3 * (idx - w) + c];
-                rhs[3 * idx + c] = alpha * primal[3 * idx + c] + div;
+                const T a = alpha * primal[3 * idx + c];
+                rhs[3 * idx + c] = neg_div ? a - div : a + div;
             }
         }
     for (uint32_t it = 0; it < iters; ++it)

@@ -87,7 +87,7 @@ int render_impl(const Scene<T>& sc, const ar_camera_desc* cd, const ar_integrato
         if (moments)
             for (size_t i = 0; i < n; ++i) mom[i] = pr[i];  // primal film
         poisson_sor(w, h, pr.data(), gx.data(), gy.data(), T(cfg->alpha), cfg->poisson_iterations, T(cfg->sor_omega),
-                    buf.data());
+                    buf.data(), (cfg->gdpt_flags & AR_GDPT_CONSISTENT_DIVERGENCE) != 0);
     } else {
         return -1;
     }

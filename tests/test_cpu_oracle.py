@@ -146,6 +146,21 @@ def test_oracle_gdpt_gradients_are_zero_on_border():
     assert np.all(img >= 0)
 
 
+def test_oracle_gdpt_divergence_sign():
+    """The reference's Poisson right-hand side (+div G) pulls the GDPT image
+    away from the PT image; the consistent sign (-div G, an opt-in extension)
+    lands on it."""
+    sc, cam = S.cornell_box(1)
+    w, h = 24, 20
+    osc = O.OracleScene(sc)
+    pt = osc.render(cam, integrator_cfg(A.INTEGRATOR_PT, spp=256, max_depth=6, seed=1), w, h)
+    ref_sign = osc.render(cam, integrator_cfg(A.INTEGRATOR_GDPT, spp=32, max_depth=6, seed=2), w, h)
+    fixed = osc.render(cam, integrator_cfg(A.INTEGRATOR_GDPT, spp=32, max_depth=6, seed=2,
+                                           gdpt_flags=A.GDPT_CONSISTENT_DIVERGENCE), w, h)
+    err = lambda x: float(np.mean(np.abs(x - pt)))
+    assert err(fixed) < 0.2 * err(ref_sign), (err(fixed), err(ref_sign))
+
+
 def test_header_symbols_exported():
     import ctypes
     from agentray import _lib

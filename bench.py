@@ -1,7 +1,7 @@
 """Benchmark driver: one JSON line on rank 0.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload served|pt_cornell|pt_served4|bdpt_room|gdpt_room|bvh]
+                    [--workload served|pt_cornell|pt_served4|bdpt_served4|bdpt_room|gdpt_room|bvh]
                     [--jobs J]
                     [--window-jobs J] [--served-jobs J]
 
@@ -24,6 +24,7 @@ Workloads (seeded synthetic inputs with the stated shapes; no dataset exists):
   pt_cornell  PT Cornell box (34 tris + quad light, 256x256, 16 spp, depth 8);
               one step = one full render.
   pt_served4  PT on served scene 4 (139k tris, 335 instances), 512x512, 16 spp.
+  bdpt_served4 BDPT on served scene 4, 512x512, 16 spp, depth 8.
   bdpt_room   BDPT on the 200k-tri room, 512x512, 64 spp, depth 10, FP64 film.
   gdpt_room   GDPT on the room, 1024x1024, 32 spp, CG Poisson to 1e-6.
   bvh         BVH micro-benchmark: 1M triangles, 16M closest-hit rays (Mrays/s).
@@ -575,10 +576,19 @@ def run_room(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_ki
     from agentray.scene_data import integrator_cfg
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    sc, cam = S.room(4)
+    sc, cam = S.served_scene(4) if args.workload == "bdpt_served4" else S.room(4)
     scene = agentray.Scene(ctx, sc)
     ntri = scene.stats()["num_triangles"]
-    if args.workload == "bdpt_room":
+    if args.workload == "bdpt_served4":
+        W = H = 512
+        spp = 16
+        integ = agentray.BidirectionalPathTracer(agentray.BdptConfig(spp=spp, max_depth=8, rr_depth=3, seed=4 + rank))
+        cfg = integrator_cfg(A.INTEGRATOR_BDPT, spp=1, max_depth=8, rr_depth=3)
+        desc = (f"bdpt_served4: BDPT+MIS on served scene 4 ({ntri} tris, 335 instances, 2 quad lights), 512x512, "
+                f"16 spp, max depth 8")
+        top = "bdpt_shadow"
+        dtype = "f32"
+    elif args.workload == "bdpt_room":
         W = H = 512
         spp = 64
         integ = agentray.BidirectionalPathTracer(agentray.BdptConfig(spp=spp, max_depth=10, rr_depth=3, seed=4 + rank,
@@ -663,7 +673,10 @@ def run_room(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_ki
                     "d2h_bytes_per_step": W * H * 3 * 4, "note": "scene resident; image returned to a host buffer"},
             "gpu_launches": int(sum(v[0] for v in prof.values()) * args.steps),
             "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peaks["hbm_gbs"],
-                         "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                         "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                         "traffic": profile_traffic({"bdpt_served4": "bdpt_shadow_served4",
+                                                     "bdpt_room": "bdpt_shadow_room",
+                                                     "gdpt_room": "pt_extend_room"}[args.workload]),
                          "peak_kind": peak_kind,
                          "bytes_model": f"{rays} rays x (48 + 32*{nodes:.2f} nodes + 36*{tris:.2f} tris) B over "
                                         f"{ln} launches; reference-traversal counts of primary/interior rays"},
@@ -767,7 +780,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="served",
-                    choices=["served", "pt_cornell", "pt_served4", "bdpt_room", "gdpt_room", "bvh"])
+                    choices=["served", "pt_cornell", "pt_served4", "bdpt_served4", "bdpt_room", "gdpt_room", "bvh"])
     ap.add_argument("--jobs", type=int, default=2000)
     ap.add_argument("--window-jobs", dest="window_jobs", type=int, default=16)
     ap.add_argument("--served-jobs", dest="served_jobs", type=int, default=160)
@@ -802,7 +815,7 @@ def main():
         run_served(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind)
     elif args.workload in ("pt_cornell", "pt_served4"):
         run_pt_cornell(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind, stream)
-    elif args.workload in ("bdpt_room", "gdpt_room"):
+    elif args.workload in ("bdpt_served4", "bdpt_room", "gdpt_room"):
         run_room(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind, stream)
     else:
         run_bvh(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind, stream)

@@ -674,7 +674,7 @@ def run_room(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_ki
             "gpu_launches": int(sum(v[0] for v in prof.values()) * args.steps),
             "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peaks["hbm_gbs"],
                          "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
-                         "traffic": profile_traffic({"bdpt_served4": "bdpt_shadow_served4",
+                         "traffic": profile_traffic({"bdpt_served4": "bdpt_served4",
                                                      "bdpt_room": "bdpt_shadow_room",
                                                      "gdpt_room": "pt_extend_room"}[args.workload]),
                          "peak_kind": peak_kind,

@@ -209,7 +209,8 @@ def run_served(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_
     built = [S.served_scene(k) for k in range(8)]
     scenes = [agentray.Scene(ctx, sd) for sd, _ in built]
     cams = [cam for _, cam in built]
-    srv = agentray.Server(ctx, film_budget_bytes=24 << 30, path_capacity=1 << 21, bdpt_batch_samples=1 << 19,
+    srv = agentray.Server(ctx, film_budget_bytes=24 << 30, path_capacity=args.path_capacity,
+                          bdpt_batch_samples=args.bdpt_batch,
                           bdpt_max_depth=8)
     W, K = max(3, args.warmup), args.steps
     per = max(1, min(args.window_jobs, n_jobs // (W + K + 1)))
@@ -329,8 +330,8 @@ def run_served(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_
                        "timed_pt_jobs": n_pt, "stream_jobs": n_jobs,
                        "stream_use": f"jobs [0, {(W + K) * per}) as W+K windows of {per}, the next "
                                      f"{len(served_jobs)} as the Poisson-arrival served run", "l2": "flushed (256 MiB write) before each window",
-                       "parallelism": f"replicas x{world}", "server": {"path_capacity": 1 << 21,
-                                                                       "bdpt_batch_samples": 1 << 19}},
+                       "parallelism": f"replicas x{world}", "server": {"path_capacity": args.path_capacity,
+                                                                       "bdpt_batch_samples": args.bdpt_batch}},
             "e2e": {"value": e2e_value, "unit": "Mpath-samples/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": int(d2h / max(1, min(2, K))),
                     "note": "scenes resident; per step the job descriptors go host->device and every image "
@@ -784,6 +785,8 @@ def main():
     ap.add_argument("--jobs", type=int, default=2000)
     ap.add_argument("--window-jobs", dest="window_jobs", type=int, default=16)
     ap.add_argument("--served-jobs", dest="served_jobs", type=int, default=160)
+    ap.add_argument("--path-capacity", dest="path_capacity", type=int, default=1 << 22)
+    ap.add_argument("--bdpt-batch", dest="bdpt_batch", type=int, default=1 << 21)
     ap.add_argument("--cpu-samples", dest="cpu_samples", type=int, default=4_000_000)
     args = ap.parse_args()
     rank, local, world = dist_env()

@@ -109,8 +109,8 @@ class Scene:
         check(lib().ar_scene_get_stats(self.handle, C.byref(s)))
         return {k: getattr(s, k) for k, _ in A.SceneStats._fields_ if not k.startswith("_")}
 
-    def rebuild(self, max_leaf_size=3, sah_bins=32, build_threads=0, bvh_width=8):
-        o = A.AccelOpts(max_leaf_size, sah_bins, build_threads, bvh_width)
+    def rebuild(self, max_leaf_size=3, sah_bins=32, build_threads=0, bvh_width=8, sah_node_cost=0.5):
+        o = A.AccelOpts(max_leaf_size, sah_bins, build_threads, bvh_width, sah_node_cost, 0)
         check(lib().ar_scene_build_accel(self.ctx.handle, self.handle, C.byref(o)))
 
     @staticmethod

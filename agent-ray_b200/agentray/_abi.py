@@ -86,7 +86,8 @@ class Hit(C.Structure):
 
 
 class AccelOpts(C.Structure):
-    _fields_ = [("max_leaf_size", u32), ("sah_bins", u32), ("build_threads", u32), ("bvh_width", u32)]
+    _fields_ = [("max_leaf_size", u32), ("sah_bins", u32), ("build_threads", u32), ("bvh_width", u32),
+                ("sah_node_cost", f32), ("_pad", u32)]
 
 
 class Tuning(C.Structure):

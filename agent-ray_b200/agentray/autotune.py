@@ -37,7 +37,7 @@ def apply(ctx, scene, entry):
     ctx.set_tuning(**entry["tuning"])
     a = entry["accel"]
     scene.rebuild(max_leaf_size=a["max_leaf_size"] or 3, sah_bins=a["sah_bins"] or 32,
-                  bvh_width=a["bvh_width"] or 8)
+                  bvh_width=a["bvh_width"] or 8, sah_node_cost=a.get("sah_node_cost") or 0.5)
 
 
 def load_cache(path):

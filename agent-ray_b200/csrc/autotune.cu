@@ -4,7 +4,7 @@
 // persistent traversal grid (blocks per SM; the block shape is fixed at 128
 // threads by the traversal launch bounds), the shading stage's block size,
 // the queue capacities (PT/GDPT path slots, BDPT batch memory) and the
-// wide-BVH build (children per node, triangles per leaf).  Coordinate
+// wide-BVH build (SAH node cost, children per node, triangles per leaf).  Coordinate
 // descent: each knob in turn is swept with the others at their current best,
 // every candidate timed as the median of `repeats` renders of the workload
 // with CUDA events on the context's stream, after one untimed render.
@@ -90,8 +90,9 @@ double time_render(ar_context* ctx, const ar_scene* sc, const ar_camera_desc& ca
 bool same_accel(const ar_accel_opts& a, const ar_accel_opts& b) {
     const auto width = [](uint32_t w) { return w ? w : 8u; };
     const auto leaf = [](uint32_t l) { return l ? l : 3u; };
+    const auto cost = [](float c) { return c > 0.f ? c : 0.5f; };
     return width(a.bvh_width) == width(b.bvh_width) && leaf(a.max_leaf_size) == leaf(b.max_leaf_size) &&
-           a.sah_bins == b.sah_bins;
+           a.sah_bins == b.sah_bins && cost(a.sah_node_cost) == cost(b.sah_node_cost);
 }
 
 void autotune(ar_context* ctx, ar_scene* sc, const ar_camera_desc& cam, const ar_tune_opts& o, ar_tune_result& r) {
@@ -125,19 +126,27 @@ void autotune(ar_context* ctx, ar_scene* sc, const ar_camera_desc& cam, const ar
     const double kGain = 0.99;  // a candidate must win by 1% to move
 
     if (o.tune_accel) {
+        const auto try_accel = [&](const ar_accel_opts& a) {
+            if (same_accel(a, best_accel)) return;
+            build_scene_accel(sc, &a);
+            const double ms = run();
+            r.candidates++;
+            if (ms < best_ms * kGain) {
+                best_ms = ms;
+                best_accel = a;
+            }
+        };
+        for (const float cost : {0.5f, 1.0f, 2.0f}) {
+            ar_accel_opts a = best_accel;
+            a.sah_node_cost = cost;
+            try_accel(a);
+        }
         for (const uint32_t width : {8u, 6u, 4u}) {
-            for (const uint32_t leaf : {3u, 2u, 1u}) {
+            for (const uint32_t leaf : {4u, 3u, 2u, 1u}) {
                 ar_accel_opts a = best_accel;
                 a.bvh_width = width;
                 a.max_leaf_size = leaf;
-                if (same_accel(a, best_accel)) continue;
-                build_scene_accel(sc, &a);
-                const double ms = run();
-                r.candidates++;
-                if (ms < best_ms * kGain) {
-                    best_ms = ms;
-                    best_accel = a;
-                }
+                try_accel(a);
             }
         }
         if (!same_accel(sc->accel, best_accel)) build_scene_accel(sc, &best_accel);

@@ -126,7 +126,7 @@ class BinaryBuilder {
         }
         const float pa = box.area();
         const float leaf_cost = float(count);
-        const float split_cost = pa > 0.f ? 1.0f + best_cost / pa : FLT_MAX;
+        const float split_cost = pa > 0.f ? opts_.node_cost + best_cost / pa : FLT_MAX;
         if (count <= opts_.max_leaf && (best_axis < 0 || leaf_cost <= split_cost)) return false;
         uint32_t* b = order + start;
         uint32_t* e = b + count;
@@ -248,7 +248,7 @@ WideBuild build_wide_bvh(const std::vector<PrimBox>& boxes, const BuildOptions& 
     WideBuild out;
     if (boxes.empty()) return out;
     BuildOptions opts = opts_in;
-    opts.max_leaf = std::max(1u, std::min(3u, opts.max_leaf));
+    opts.max_leaf = std::max(1u, std::min(4u, opts.max_leaf));  // 8 leaves x 4 fill the 32-bit triangle mask
     opts.width = std::max(2u, std::min(8u, opts.width));
     std::vector<BinNode> bn;
     std::vector<uint32_t> order;

@@ -18,10 +18,11 @@ struct PrimBox {
 };
 
 struct BuildOptions {
-    uint32_t max_leaf = 3;  // 1..3
+    uint32_t max_leaf = 3;  // 1..4
     uint32_t bins = 32;
     uint32_t threads = 0;   // 0: all hardware threads
     uint32_t width = 8;     // children per wide node, 2..8
+    float node_cost = 0.5f; // SAH: a node visit relative to one triangle test
 };
 
 struct WideBuild {

@@ -96,6 +96,7 @@ void build_scene_accel(ar_scene* s, const ar_accel_opts* o) {
         if (o->max_leaf_size) bo.max_leaf = o->max_leaf_size;
         if (o->sah_bins) bo.bins = o->sah_bins;
         if (o->bvh_width) bo.width = o->bvh_width;
+        if (o->sah_node_cost > 0.f) bo.node_cost = o->sah_node_cost;
         bo.threads = o->build_threads;
     }
     std::vector<WideNode> nodes;

@@ -67,6 +67,22 @@ def load_peaks():
     return PEAKS_FALLBACK, "fallback"
 
 
+def max_over_ranks(dist, value, device):
+    """The job's time: the largest per-rank device time (every rank calls this
+    at the same point; `dist` is None on one process)."""
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def rank_stream(n_jobs, rank):
+    """Each rank serves its own seeded job stream (weak scaling)."""
+    import agentray.scenes as S
+    return S.served_stream(n_jobs, seed=5 + 1000 * rank)
+
+
 def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
 
@@ -205,7 +221,7 @@ def run_served(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_
     import agentray.scenes as S
 
     n_jobs = args.jobs
-    stream = S.served_stream(n_jobs, seed=5 + 1000 * rank)
+    stream = rank_stream(n_jobs, rank)
     built = [S.served_scene(k) for k in range(8)]
     scenes = [agentray.Scene(ctx, sd) for sd, _ in built]
     cams = [cam for _, cam in built]
@@ -262,10 +278,7 @@ def run_served(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_
             ms_list.append(ms)
             samples_total += smp
     total_ms = sum(ms_list)
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    value = world * samples_total / (float(t.item()) / 1e3) / 1e6
+    value = world * samples_total / (max_over_ranks(dist, total_ms, "cuda") / 1e3) / 1e6
     capacity_sps = samples_total / (total_ms / 1e3)
 
     # e2e: the first two timed windows again with images returned to host
@@ -506,11 +519,7 @@ def run_pt_cornell(args, rank, local, world, torch, ctx, barrier, dist, peaks, p
     torch.cuda.synchronize()
     ctx.profile(False)
     prof = ctx.profile_read()
-    total_ms = sum(a.elapsed_time(b) for a, b in step_ms)
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
+    total_ms = max_over_ranks(dist, sum(a.elapsed_time(b) for a, b in step_ms), "cuda")
     stats = ctx.render_stats()
     samples = W * H * spp
     value = world * samples * args.steps / (total_ms / 1e3) / 1e6
@@ -627,11 +636,7 @@ def run_room(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_ki
             e1.record(stream)
             evs.append((e0, e1))
         torch.cuda.synchronize()
-    total_ms = sum(a.elapsed_time(b) for a, b in evs)
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
+    total_ms = max_over_ranks(dist, sum(a.elapsed_time(b) for a, b in evs), "cuda")
     samples = W * H * spp
     value = world * samples * args.steps / (total_ms / 1e3) / 1e6
     stats = ctx.render_stats()
@@ -714,7 +719,7 @@ def run_bvh(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kin
             b.record(stream)
             ev.append((a, b))
         torch.cuda.synchronize()
-    total_ms = sum(a.elapsed_time(b) for a, b in ev)
+    total_ms = max_over_ranks(dist, sum(a.elapsed_time(b) for a, b in ev), "cuda")
     value = world * n_rays * args.steps / (total_ms / 1e3) / 1e6
     if rank == 0:
         import oracle as O

@@ -223,3 +223,16 @@ def test_bdpt_statistically_equal_to_independent_oracle(ctx):
     r = np.stack([osc.render(cam, integrator_cfg(A.INTEGRATOR_BDPT, spp=16, max_depth=6, seed=500 + k), w, h,
                              sampler=O.SAMPLER_COUNTER) for k in range(8)])
     assert welch_fail_fraction(g, r) < 0.01
+
+
+def test_pt_furnace_analytic(ctx):
+    """Point light at the centre of a closed Lambertian sphere (albedo 0.5):
+    one bounce gives albedo/pi * I/r^2, D bounces the geometric series."""
+    import math
+    sc, cam = S.furnace(albedo=0.5)
+    one = _render_gpu(ctx, sc, cam, integrator_cfg(A.INTEGRATOR_PT, spp=2, max_depth=1, seed=1), 16, 16)
+    assert np.allclose(one, 0.5 / math.pi, rtol=0.02)
+    many = _render_gpu(ctx, sc, cam, integrator_cfg(A.INTEGRATOR_PT, spp=256, max_depth=4, rr_depth=10, seed=2),
+                       16, 16)
+    expect = 0.5 / math.pi * sum(0.5 ** k for k in range(4))
+    assert abs(many.mean() - expect) / expect < 0.02

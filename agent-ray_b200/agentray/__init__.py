@@ -25,7 +25,8 @@ from .scene_data import Camera, Light, Material, Mesh, Object, SceneData, integr
 
 __all__ = ["Context", "Scene", "Camera", "Film", "PathTracer", "PathTracerConfig", "BidirectionalPathTracer",
            "BdptConfig", "GradientDomainPathTracer", "GdptConfig", "SceneData", "Mesh", "Object", "Material",
-           "Light", "AgentRayError", "integrator_cfg", "lib", "Server", "poisson_reconstruct"]
+           "Light", "AgentRayError", "integrator_cfg", "lib", "Server", "poisson_reconstruct", "film_to_rgb8",
+           "write_png"]
 
 
 class Context:
@@ -168,16 +169,62 @@ class Scene:
 class Film:
     """Linear HDR film (src/film.rs), already divided by spp."""
 
-    def __init__(self, rgb: np.ndarray, width: int, height: int):
+    def __init__(self, rgb: np.ndarray, width: int, height: int, ctx=None):
         self.rgb = rgb.reshape(height, width, 3)
         self.width = width
         self.height = height
+        self.ctx = ctx
 
     def to_hdr_vec(self):
         return self.rgb.reshape(-1, 3)
 
     def get_pixel(self, x, y):
         return self.rgb[y, x]
+
+    def to_rgb_image(self, tone_mapper=A.TONEMAP_CLAMP, gamma=2.2, scale=1.0, white_point=1.0):
+        """Film::to_rgb_image (src/film.rs:276-302) on the GPU: (H, W, 3) uint8."""
+        return film_to_rgb8(self.ctx, self.rgb, tone_mapper, gamma, scale, white_point)
+
+    def save_png(self, path, tone_mapper=A.TONEMAP_CLAMP, gamma=2.2, scale=1.0, white_point=1.0):
+        write_png(path, self.to_rgb_image(tone_mapper, gamma, scale, white_point))
+
+
+def film_to_rgb8(ctx, hdr, tone_mapper=A.TONEMAP_CLAMP, gamma=2.2, scale=1.0, white_point=1.0):
+    """Tone-maps an (H, W, 3) float32 image (host array or CUDA tensor) to
+    8-bit RGB with ar_film_to_rgb8; returns a host array, or a CUDA uint8
+    tensor for a CUDA input."""
+    if ctx is None:
+        raise ValueError("a Context is needed to tone-map on the GPU")
+    if not isinstance(hdr, np.ndarray):
+        import torch
+        h, w = hdr.shape[0], hdr.shape[1]
+        out = torch.empty((h, w, 3), dtype=torch.uint8, device=hdr.device)
+        check(lib().ar_film_to_rgb8(ctx.handle, hdr.data_ptr(), w, h, tone_mapper, white_point, gamma, scale,
+                                    out.data_ptr(), 1))
+        return out
+    x = np.ascontiguousarray(hdr, np.float32)
+    h, w = x.shape[0], x.shape[1]
+    out = np.empty((h, w, 3), np.uint8)
+    check(lib().ar_film_to_rgb8(ctx.handle, x.ctypes.data, w, h, tone_mapper, white_point, gamma, scale,
+                                out.ctypes.data, 0))
+    return out
+
+
+def write_png(path, rgb8):
+    """Writes an (H, W, 3) uint8 image as an 8-bit RGB PNG (zlib, no filter)."""
+    import struct
+    import zlib
+    h, w, _ = rgb8.shape
+    raw = b"".join(b"\x00" + np.ascontiguousarray(rgb8[y]).tobytes() for y in range(h))
+
+    def chunk(tag, data):
+        c = struct.pack(">I", len(data)) + tag + data
+        return c + struct.pack(">I", zlib.crc32(tag + data) & 0xFFFFFFFF)
+    with open(path, "wb") as f:
+        f.write(b"\x89PNG\r\n\x1a\n")
+        f.write(chunk(b"IHDR", struct.pack(">IIBBBBB", w, h, 8, 2, 0, 0, 0)))
+        f.write(chunk(b"IDAT", zlib.compress(raw, 6)))
+        f.write(chunk(b"IEND", b""))
 
 
 @dataclass
@@ -248,7 +295,7 @@ class _Integrator:
         buf = np.empty(width * height * 3, np.float32) if out is None else out
         check(lib().ar_render(scene.ctx.handle, scene.handle, C.byref(cam), C.byref(cfg), width, height,
                               buf.ctypes.data, 0))
-        return Film(buf, width, height)
+        return Film(buf, width, height, scene.ctx)
 
 
 class PathTracer(_Integrator):

@@ -32,6 +32,9 @@ POISSON_CG = 1
 FILM_F32 = 0
 FILM_F64 = 1
 GDPT_CONSISTENT_DIVERGENCE = 1
+TONEMAP_CLAMP = 0
+TONEMAP_REINHARD = 1
+TONEMAP_REINHARD_EXTENDED = 2
 
 u32 = C.c_uint32
 f32 = C.c_float

@@ -293,6 +293,20 @@ int ar_render(ar_context* ctx, const ar_scene* scene, const ar_camera_desc* came
               const ar_integrator_cfg* cfg, uint32_t width, uint32_t height,
               float* out_rgb, uint32_t out_on_device);
 
+/* ---- film output (src/film.rs:136-302) ---- */
+
+enum ar_tone_mapper {
+    AR_TONEMAP_CLAMP = 0,            /* ToneMapper::Clamp */
+    AR_TONEMAP_REINHARD = 1,         /* ToneMapper::Reinhard (luminance-preserving) */
+    AR_TONEMAP_REINHARD_EXTENDED = 2 /* ToneMapper::ReinhardExtended { white_point } */
+};
+
+/* Film::to_rgb_image: scale, tone-map, encode with 1/gamma and quantise to
+ * 8-bit RGB (W*H*3 bytes, row-major from the top-left).  `hdr_rgb` and
+ * `out_rgb8` are host pointers, or device pointers with on_device = 1. */
+int ar_film_to_rgb8(ar_context* ctx, const float* hdr_rgb, uint32_t width, uint32_t height, uint32_t tone_mapper,
+                    float white_point, float gamma, float scale, uint8_t* out_rgb8, uint32_t on_device);
+
 /* screened_poisson_reconstruct (src/integrators/gradient_domain_pt.rs:449-630):
  * reconstructs an image from interleaved-RGB primal and forward-difference
  * gradient films (W*H*3 f32 each) with cfg->alpha and cfg->poisson_solver

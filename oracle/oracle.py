@@ -42,6 +42,7 @@ def lib():
         lb.oracle_counter_u01.argtypes = [u64, u32, u32, u32, u32, vp]
         lb.oracle_xoshiro_f32.argtypes = [u32, u32, u32, vp]
         lb.oracle_blas_stats.argtypes = [vp, u32, vp]
+        lb.oracle_film_to_rgb8.argtypes = [vp, u32, u32, u32, C.c_float, C.c_float, C.c_float, vp]
         _lib = lb
     return _lib
 
@@ -152,3 +153,13 @@ def xoshiro_f32(px, py, n):
     out = np.empty(n, np.float32)
     lib().oracle_xoshiro_f32(px, py, n, _p(out))
     return out
+
+
+def film_to_rgb8(hdr, tone_mapper=0, white_point=1.0, gamma=2.2, scale=1.0):
+    """Film::to_rgb_image on an (H, W, 3) float32 image -> (H, W, 3) uint8."""
+    h, w, _ = hdr.shape
+    x = np.ascontiguousarray(hdr, np.float32)
+    out = np.empty((h, w, 3), np.uint8)
+    lib().oracle_film_to_rgb8(_p(x), w, h, tone_mapper, white_point, gamma, scale, _p(out))
+    return out
+

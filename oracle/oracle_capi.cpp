@@ -1,6 +1,7 @@
 // ORACLE — test infrastructure only.  C entry points over the CPU restatement
 // of agent-ray (ar_*.hpp) for the pytest suite, __graft_entry__.smoke() and the
 // CPU-baseline leg of bench.py.  PARITY UNPINNED (see ar_math.hpp).
+#include <cmath>
 #include <chrono>
 #include <cstdio>
 #include <memory>
@@ -157,6 +158,35 @@ int oracle_poisson_exact_f64(uint32_t w, uint32_t h, const double* primal, const
 int oracle_counter_u01(uint64_t seed, uint32_t pixel, uint32_t sample, uint32_t dim0, uint32_t n, float* out) {
     uint64_t key = counter_key(seed, pixel, sample);
     for (uint32_t i = 0; i < n; ++i) out[i] = counter_u01(key, dim0 + i);
+    return 0;
+}
+
+// Film::to_rgb_image (src/film.rs:276-302) with tonemap_pixel (:153-181):
+// scale, tone-map, clamp, powf(1/gamma), (x * 255 + 0.5).min(255) as u8.
+// Every operation is a separate f32 rounding in the reference's order.
+int oracle_film_to_rgb8(const float* hdr, uint32_t w, uint32_t h, uint32_t tm, float white_point, float gamma,
+                        float scale, uint8_t* out) {
+    const float inv_gamma = 1.0f / gamma;
+    const size_t n = size_t(w) * h;
+    for (size_t i = 0; i < n; ++i) {
+        float c[3] = {hdr[3 * i] * scale, hdr[3 * i + 1] * scale, hdr[3 * i + 2] * scale};
+        float s = 1.0f;
+        const float lum = (0.2126f * c[0] + 0.7152f * c[1]) + 0.0722f * c[2];
+        if (tm == 1) {
+            s = lum > 1e-6f ? (lum / (1.0f + lum)) / lum : 1.0f / (1.0f + lum);
+        } else if (tm == 2) {
+            const float lw2 = white_point * white_point;
+            const float mapped = (lum * (1.0f + lum / lw2)) / (1.0f + lum);
+            s = lum > 1e-6f ? mapped / lum : 1.0f;
+        }
+        for (int k = 0; k < 3; ++k) {
+            float m = tm == 0 ? c[k] : c[k] * s;
+            m = std::min(std::max(m, 0.0f), 1.0f);  // Vec3A::clamp(ZERO, ONE)
+            const float e = std::pow(m, inv_gamma);
+            const float v = std::min(e * 255.0f + 0.5f, 255.0f);
+            out[3 * i + k] = v > 0.0f ? uint8_t(v) : uint8_t(0);  // Rust `as u8` saturates
+        }
+    }
     return 0;
 }
 

@@ -236,3 +236,21 @@ def test_pt_furnace_analytic(ctx):
                        16, 16)
     expect = 0.5 / math.pi * sum(0.5 ** k for k in range(4))
     assert abs(many.mean() - expect) / expect < 0.02
+
+
+@pytest.mark.parametrize("tm,wp", [(A.TONEMAP_CLAMP, 1.0), (A.TONEMAP_REINHARD, 1.0),
+                                   (A.TONEMAP_REINHARD_EXTENDED, 4.0)])
+def test_film_to_rgb8_matches_oracle(ctx, tm, wp):
+    # Bytes: equal except where CUDA's powf and the host's differ by an ulp on a
+    # rounding boundary (at most 1 LSB, on < 0.1% of the values).
+    sc, cam = S.cornell_box(1)
+    film = agentray.PathTracer(agentray.PathTracerConfig(spp=4, seed=3)).render(agentray.Scene(ctx, sc), cam, 64, 48)
+    hdr = film.rgb.copy()
+    for scale in (1.0, 3.0):
+        g = agentray.film_to_rgb8(ctx, hdr, tm, 2.2, scale, wp)
+        r = O.film_to_rgb8(hdr, tm, wp, 2.2, scale)
+        d = np.abs(g.astype(int) - r.astype(int))
+        assert d.max() <= 1 and (d > 0).mean() < 1e-3, (d.max(), (d > 0).mean())
+    import torch
+    dev = agentray.film_to_rgb8(ctx, torch.from_numpy(hdr).cuda(), tm, 2.2, 1.0, wp)
+    np.testing.assert_array_equal(dev.cpu().numpy(), agentray.film_to_rgb8(ctx, hdr, tm, 2.2, 1.0, wp))

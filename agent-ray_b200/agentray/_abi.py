@@ -17,6 +17,7 @@ AR_ERR_INTERNAL = -8
 
 MATERIAL_LAMBERTIAN = 0
 MATERIAL_CONDUCTOR = 1
+MATERIAL_DIELECTRIC = 2
 LIGHT_POINT = 0
 LIGHT_QUAD = 1
 LIGHT_DIST_NONE = 0
@@ -53,7 +54,7 @@ class ObjectDesc(C.Structure):
 
 class MaterialDesc(C.Structure):
     _fields_ = [("kind", u32), ("emitter_light", C.c_int32), ("albedo", f32 * 3), ("f0", f32 * 3),
-                ("roughness", f32), ("_pad", f32)]
+                ("roughness", f32), ("eta", f32)]
 
 
 class LightDesc(C.Structure):

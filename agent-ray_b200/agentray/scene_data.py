@@ -30,6 +30,7 @@ class Material:
     f0: tuple = (0.9, 0.9, 0.9)
     roughness: float = 0.3
     emitter_light: int = -1
+    eta: float = 1.5  # dielectric interior index of refraction
 
 
 @dataclass
@@ -142,6 +143,7 @@ class SceneData:
             mats_d[i].albedo[:] = [float(x) for x in m.albedo]
             mats_d[i].f0[:] = [float(x) for x in m.f0]
             mats_d[i].roughness = float(m.roughness)
+            mats_d[i].eta = float(m.eta)
         lights_d = (A.LightDesc * max(1, len(self.lights)))()
         for i, l in enumerate(self.lights):
             lights_d[i].kind = l.kind

@@ -99,9 +99,11 @@ def add_quad_light(sc, corner, e1, e2, radiance, visible=True):
 
 
 # ------------------------------------------------------------------ scenes --
-def cornell_box(seed=1, light_radiance=15.0, point_light=False):
+def cornell_box(seed=1, light_radiance=15.0, point_light=False, glass=False):
     """Config-1 Cornell box: 5 walls (10 tris) + 2 rotated boxes (24 tris) and a
-    0.25 x 0.25 quad light of radiance 15 just below the ceiling."""
+    0.25 x 0.25 quad light of radiance 15 just below the ceiling.  glass=True
+    makes the tall box a rough dielectric (eta 1.5, alpha 0.2) and adds a
+    dielectric icosphere (eta 1.33, alpha 0.05)."""
     rng = np.random.default_rng(seed)
     sc = SceneData(A.LIGHT_DIST_POWER)
     walls = [((0, 0, 0), (0, 0, 1), (1, 0, 0)),   # floor
@@ -114,11 +116,18 @@ def cornell_box(seed=1, light_radiance=15.0, point_light=False):
         mat = sc.add_material(Material(A.MATERIAL_LAMBERTIAN, albedo=tuple(rng.uniform(0.2, 0.8, 3))))
         sc.add_object(Object(m, [mat]))
     cube = sc.add_mesh(unit_cube_mesh())
-    for (tx, ty, tz), deg, (sx, sy, sz) in [((0.33, 0.3, 0.35), 15.0, (0.3, 0.6, 0.3)),
-                                            ((0.67, 0.15, 0.62), -18.0, (0.3, 0.3, 0.3))]:
+    for k, ((tx, ty, tz), deg, (sx, sy, sz)) in enumerate([((0.33, 0.3, 0.35), 15.0, (0.3, 0.6, 0.3)),
+                                                          ((0.67, 0.15, 0.62), -18.0, (0.3, 0.3, 0.3))]):
         mat = sc.add_material(Material(A.MATERIAL_LAMBERTIAN, albedo=tuple(rng.uniform(0.2, 0.8, 3))))
+        if glass and k == 0:
+            mat = sc.add_material(Material(A.MATERIAL_DIELECTRIC, roughness=0.2, eta=1.5))
         xf, inv = trs((tx, ty, tz), rot_y(deg), (sx, sy, sz))
         sc.add_object(Object(cube, [mat], xf, inv))
+    if glass:
+        sph = sc.add_mesh(icosphere(3))
+        mat = sc.add_material(Material(A.MATERIAL_DIELECTRIC, roughness=0.05, eta=1.33))
+        xf, inv = trs((0.7, 0.45, 0.6), None, (0.14, 0.14, 0.14))
+        sc.add_object(Object(sph, [mat], xf, inv))
     if point_light:
         sc.add_light(Light(A.LIGHT_POINT, (0.5, 0.9, 0.5), (light_radiance * 0.0625,) * 3))
     else:

@@ -6,6 +6,7 @@
 //   Onb                          src/geometry.rs:218-244
 //   Lambertian                   src/surfaces/lambertian.rs:35-64
 //   ConductorBsdf (GGX)          src/surfaces/microfacet.rs:14-152
+//   DielectricBsdf (GGX glass)   src/surfaces/microfacet.rs:155-307, src/surfaces.rs:86-123
 //   PointLight                   src/lights/point.rs:48-100
 //   Uniform/PowerLightDistribution src/lights.rs:136-235
 //   PinholeCamera                src/cameras.rs:146-248
@@ -107,7 +108,7 @@ struct MatView {
     uint32_t kind;
     int32_t emitter;
     float albedo[3], f0[3];
-    float alpha;
+    float alpha, eta;
 };
 __device__ __forceinline__ MatView load_mat(const DevScene& sc, uint32_t m) {
     const MaterialRecord& r = sc.materials[m];
@@ -116,10 +117,87 @@ __device__ __forceinline__ MatView load_mat(const DevScene& sc, uint32_t m) {
     v.emitter = r.emitter;
     for (int k = 0; k < 3; ++k) { v.albedo[k] = r.albedo[k]; v.f0[k] = r.f0[k]; }
     v.alpha = r.alpha;
+    v.eta = r.eta;
     return v;
 }
 
+// ---- DielectricBsdf (microfacet.rs:155-307) with fresnel_dielectric and
+// refract (surfaces.rs:86-123); operation order as in the reference ----
+__device__ __forceinline__ float fresnel_dielectric(float cos_theta_i, float eta) {
+    float ci = fminf(fmaxf(cos_theta_i, -1.0f), 1.0f);
+    if (ci < 0.0f) {
+        ci = -ci;
+        eta = 1.0f / eta;
+    }
+    const float sin2_t = (eta * eta) * (1.0f - ci * ci);
+    if (sin2_t >= 1.0f) return 1.0f;
+    const float ct = sqrtf(1.0f - sin2_t);
+    const float r_par = (eta * ci - ct) / (eta * ci + ct);
+    const float r_per = (ci - eta * ct) / (ci + eta * ct);
+    return 0.5f * (r_par * r_par + r_per * r_per);
+}
+__device__ __forceinline__ bool refract_dir(f3 v, f3 n, float eta, f3& out) {
+    const float cos_i = dot(n, v);
+    const float sin2_t = (eta * eta) * (1.0f - cos_i * cos_i);
+    if (sin2_t >= 1.0f) return false;
+    const float cos_t = sqrtf(1.0f - sin2_t);
+    out = (-v) * eta + n * (eta * cos_i - cos_t);
+    return true;
+}
+__device__ __forceinline__ float ggx_g2(float a, f3 wi, f3 wo) {
+    return 1.0f / ((1.0f + ggx_lambda(a, wi)) + ggx_lambda(a, wo));
+}
+// Refraction half-vector -(wo + wi*eta).normalize(), turned to wo's side.
+__device__ __forceinline__ f3 refraction_half(f3 wi, f3 wo, float eta) {
+    f3 h = -normalize(wo + wi * eta);
+    if (h.z * wo.z < 0.f) h = -h;
+    return h;
+}
+__device__ __forceinline__ f3 dielectric_eval(const MatView& m, f3 wi, f3 wo) {
+    const float cos_wo = fabsf(wo.z), cos_wi = fabsf(wi.z);
+    if (cos_wo == 0.f || cos_wi == 0.f) return mk(0.f, 0.f, 0.f);
+    float v;
+    if (same_hemi(wi, wo)) {
+        const f3 h = normalize(wi + wo);
+        const float f = fresnel_dielectric(fabsf(dot(wi, h)), m.eta);
+        v = ((f * ggx_d(m.alpha, h)) * ggx_g2(m.alpha, wi, wo)) / ((4.0f * cos_wi) * cos_wo);
+    } else {
+        const float eta = wo.z > 0.f ? m.eta : 1.0f / m.eta;
+        const f3 h = refraction_half(wi, wo, eta);
+        const float woh = dot(wo, h), wih = dot(wi, h);
+        if (woh == 0.f || wih == 0.f) return mk(0.f, 0.f, 0.f);
+        const float f = 1.0f - fresnel_dielectric(fabsf(wih), m.eta);
+        const float d = ggx_d(m.alpha, h), g = ggx_g2(m.alpha, wi, wo);
+        const float s = woh + eta * wih;
+        const float denom = s * s;
+        if (denom == 0.f) return mk(0.f, 0.f, 0.f);
+        const float eta2 = eta * eta;
+        v = ((((f * d) * g) * eta2) * fabsf(woh)) * fabsf(wih) / ((cos_wi * cos_wo) * denom);
+    }
+    return mk(v, v, v);
+}
+__device__ __forceinline__ float dielectric_pdf(const MatView& m, f3 wi, f3 wo) {
+    if (fabsf(wo.z) == 0.f || fabsf(wi.z) == 0.f) return 0.f;
+    if (same_hemi(wi, wo)) {
+        const f3 h = normalize(wi + wo);
+        const float whwi = fabsf(dot(wi, h));
+        if (whwi == 0.f) return 0.f;
+        const float f = fresnel_dielectric(fabsf(dot(wo, h)), m.eta);
+        return ((f * ggx_d(m.alpha, h)) * fabsf(h.z)) / (4.0f * whwi);
+    }
+    const float eta = wo.z > 0.f ? m.eta : 1.0f / m.eta;
+    const f3 h = refraction_half(wi, wo, eta);
+    const float woh = dot(wo, h), wih = dot(wi, h);
+    if (woh == 0.f || wih == 0.f) return 0.f;
+    const float s = woh + eta * wih;
+    const float denom = s * s;
+    if (denom == 0.f) return 0.f;
+    const float f = 1.0f - fresnel_dielectric(fabsf(woh), m.eta);
+    return (((((f * ggx_d(m.alpha, h)) * fabsf(h.z)) * eta) * eta) * fabsf(wih)) / denom;
+}
+
 __device__ __forceinline__ f3 bsdf_eval(const MatView& m, f3 wi, f3 wo) {
+    if (m.kind == AR_MATERIAL_DIELECTRIC) return dielectric_eval(m, wi, wo);
     if (!same_hemi(wi, wo)) return mk(0.f, 0.f, 0.f);
     if (m.kind == AR_MATERIAL_LAMBERTIAN) return mk(m.albedo[0] * kInvPi, m.albedo[1] * kInvPi, m.albedo[2] * kInvPi);
     float ci = fabsf(wi.z), co = fabsf(wo.z);
@@ -131,6 +209,7 @@ __device__ __forceinline__ f3 bsdf_eval(const MatView& m, f3 wi, f3 wo) {
     return f * (d * g / ((4.0f * ci) * co));
 }
 __device__ __forceinline__ float bsdf_pdf(const MatView& m, f3 wi, f3 wo) {
+    if (m.kind == AR_MATERIAL_DIELECTRIC) return dielectric_pdf(m, wi, wo);
     if (!same_hemi(wi, wo)) return 0.f;
     if (m.kind == AR_MATERIAL_LAMBERTIAN) return fabsf(wi.z) * kInvPi;
     f3 h = normalize(wi + wo);
@@ -138,8 +217,10 @@ __device__ __forceinline__ float bsdf_pdf(const MatView& m, f3 wi, f3 wo) {
     if (whwi == 0.f) return 0.f;
     return ggx_d(m.alpha, h) * fabsf(h.z) / (4.0f * whwi);
 }
-// Returns false when the reference returns None.
-__device__ __forceinline__ bool bsdf_sample(const MatView& m, f3 wo, float ux, float uy, f3& wi, float& pdf, f3& f) {
+// Returns false when the reference returns None.  u_sel picks the
+// dielectric's lobe (reflection when u_sel < F); the other BSDFs ignore it.
+__device__ __forceinline__ bool bsdf_sample(const MatView& m, f3 wo, float u_sel, float ux, float uy, f3& wi,
+                                            float& pdf, f3& f) {
     if (m.kind == AR_MATERIAL_LAMBERTIAN) {
         wi = cosine_hemisphere(ux, uy);
         if (wo.z < 0.f) wi.z = -wi.z;
@@ -155,6 +236,15 @@ __device__ __forceinline__ bool bsdf_sample(const MatView& m, f3 wo, float ux, f
     float phi = (2.0f * kPi) * uy;
     f3 h = mk(sh * cosf(phi), sh * sinf(phi), ch);
     if (h.z * wo.z < 0.f) h = -h;
+    if (m.kind == AR_MATERIAL_DIELECTRIC && !(u_sel < fresnel_dielectric(fabsf(dot(wo, h)), m.eta))) {
+        const float eta = wo.z > 0.f ? 1.0f / m.eta : m.eta;
+        if (!refract_dir(wo, h, eta, wi)) return false;
+        if (same_hemi(wi, wo)) return false;
+        pdf = bsdf_pdf(m, wi, wo);
+        if (pdf == 0.f) return false;
+        f = bsdf_eval(m, wi, wo);
+        return true;
+    }
     wi = -wo + (h * 2.0f) * dot(wo, h);
     if (!same_hemi(wi, wo)) return false;
     pdf = bsdf_pdf(m, wi, wo);

@@ -76,7 +76,8 @@ struct alignas(16) MaterialRecord {
     float albedo[3];
     float f0[3];
     float alpha;
-    float pad[3];
+    float eta;  // dielectric interior IOR
+    float pad[2];
 };
 
 struct alignas(16) LightRecord {

@@ -409,11 +409,11 @@ __global__ void __launch_bounds__(256) k_bd_vertex(BdParams P, uint32_t depth) {
                 const uint64_t key = counter_key(J.seed, uint32_t(g % npix), uint32_t(g / npix));
                 uint32_t d = P.dim[q];
                 const f3 wo_l = to_local(s.onb, -rd);
-                d++;  // u_sel (unused by these BSDFs)
+                const float usel = counter_u01(key, d++);
                 const float ux = counter_u01(key, d++), uy = counter_u01(key, d++);
                 f3 wi, f;
                 float pdf;
-                if (bsdf_sample(m, wo_l, ux, uy, wi, pdf, f) && pdf != 0.f && !is_zero(f)) {
+                if (bsdf_sample(m, wo_l, usel, ux, uy, wi, pdf, f) && pdf != 0.f && !is_zero(f)) {
                     thr = thr * ((f * fabsf(wi.z)) / pdf);
                     const float pdf_rev_dir = bsdf_pdf(m, wo_l, wi);
                     P.vb[pi].w = pdf_sa_to_area(pdf_rev_dir, s.p, prev_p, prev_n);

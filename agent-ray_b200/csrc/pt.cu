@@ -269,12 +269,12 @@ __global__ void __launch_bounds__(256) k_shade(EngineDev E, int q) {
                     }
                 }
                 // BSDF sampling, Russian roulette, spawn (:119-153).
-                dim++;  // u_sel of Bsdf::sample (unused by these BSDFs)
+                const float usel = counter_u01(key, dim++);
                 const float udx = counter_u01(key, dim++);
                 const float udy = counter_u01(key, dim++);
                 f3 wi, f;
                 float pdf;
-                if (bsdf_sample(m, wo_l, udx, udy, wi, pdf, f) && pdf != 0.f && !is_zero(f)) {
+                if (bsdf_sample(m, wo_l, usel, udx, udy, wi, pdf, f) && pdf != 0.f && !is_zero(f)) {
                     thr = thr * ((f * fabsf(wi.z)) / pdf);
                     prev_pdf = pdf;
                     bool alive = true;

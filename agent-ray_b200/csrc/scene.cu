@@ -288,7 +288,9 @@ void create_scene(ar_context* ctx, const ar_scene_desc* d, ar_scene** out) {
     s->materials_h.resize(d->num_materials);
     for (uint32_t i = 0; i < d->num_materials; ++i) {
         const auto& m = d->materials[i];
-        AR_REQUIRE(m.kind <= AR_MATERIAL_CONDUCTOR, AR_ERR_INVALID_ARGUMENT, "unknown material kind");
+        AR_REQUIRE(m.kind <= AR_MATERIAL_DIELECTRIC, AR_ERR_INVALID_ARGUMENT, "unknown material kind");
+        AR_REQUIRE(m.kind != AR_MATERIAL_DIELECTRIC || m.eta > 0.f, AR_ERR_INVALID_ARGUMENT,
+                   "dielectric eta must be positive");
         AR_REQUIRE(m.emitter_light < int32_t(d->num_lights), AR_ERR_INVALID_ARGUMENT, "emitter_light out of range");
         if (m.emitter_light >= 0)
             AR_REQUIRE(d->lights[m.emitter_light].kind == AR_LIGHT_QUAD, AR_ERR_INVALID_ARGUMENT,
@@ -298,6 +300,7 @@ void create_scene(ar_context* ctx, const ar_scene_desc* d, ar_scene** out) {
         r.emitter = m.emitter_light;
         for (int k = 0; k < 3; ++k) { r.albedo[k] = m.albedo[k]; r.f0[k] = m.f0[k]; }
         r.alpha = std::min(1.0f, std::max(1e-3f, m.roughness));
+        r.eta = m.eta;
         s->materials_h[i] = r;
     }
     // lights + distribution (src/lights.rs:171-235)

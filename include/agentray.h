@@ -86,7 +86,8 @@ typedef struct ar_object_desc {
 
 enum ar_material_kind {
     AR_MATERIAL_LAMBERTIAN = 0,      /* src/surfaces/lambertian.rs */
-    AR_MATERIAL_CONDUCTOR = 1        /* src/surfaces/microfacet.rs:86-152 (GGX) */
+    AR_MATERIAL_CONDUCTOR = 1,       /* src/surfaces/microfacet.rs:86-152 (GGX) */
+    AR_MATERIAL_DIELECTRIC = 2       /* src/surfaces/microfacet.rs:155-307 (rough GGX glass) */
 };
 
 typedef struct ar_material_desc {
@@ -95,8 +96,8 @@ typedef struct ar_material_desc {
                                         `emitter_light` (area-light extension); -1 otherwise */
     float albedo[3];                 /* Lambertian albedo (constant texture) */
     float f0[3];                     /* conductor reflectance at normal incidence */
-    float roughness;                 /* conductor GGX alpha, clamped to [1e-3, 1] */
-    float _pad;
+    float roughness;                 /* conductor / dielectric GGX alpha, clamped to [1e-3, 1] */
+    float eta;                       /* dielectric interior index of refraction (> 0) */
 } ar_material_desc;
 
 enum ar_light_kind {

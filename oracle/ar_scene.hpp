@@ -97,6 +97,33 @@ inline V3<T> ggx_sample_wh(T alpha, V3<T> wo, V2<T> u) {
     return h;
 }
 
+// src/surfaces.rs:86-101
+template <class T>
+inline T fresnel_dielectric(T cos_theta_i, T eta) {
+    T ci = cos_theta_i < T(-1) ? T(-1) : (cos_theta_i > T(1) ? T(1) : cos_theta_i);
+    if (ci < T(0)) {
+        ci = -ci;
+        eta = T(1) / eta;
+    }
+    T sin2_t = (eta * eta) * (T(1) - ci * ci);
+    if (sin2_t >= T(1)) return T(1);  // total internal reflection
+    T ct = std::sqrt(T(1) - sin2_t);
+    T r_par = (eta * ci - ct) / (eta * ci + ct);
+    T r_per = (ci - eta * ct) / (ci + eta * ct);
+    return T(0.5f) * (r_par * r_par + r_per * r_per);
+}
+
+// src/surfaces.rs:115-123: eta * (-v) + n * (eta * cos_i - cos_t), or None on TIR
+template <class T>
+inline bool refract(V3<T> v, V3<T> n, T eta, V3<T>& out) {
+    T cos_i = dot(n, v);
+    T sin2_t = (eta * eta) * (T(1) - cos_i * cos_i);
+    if (sin2_t >= T(1)) return false;
+    T cos_t = std::sqrt(T(1) - sin2_t);
+    out = (-v) * eta + n * (eta * cos_i - cos_t);
+    return true;
+}
+
 template <class T>
 struct BsdfSample {
     V3<T> wi;
@@ -111,8 +138,59 @@ struct Material {
     int32_t emitter;      // quad light index or -1 (EXTENSION)
     V3<T> albedo, f0;
     T alpha;
+    T eta;                // DielectricBsdf interior IOR
+
+    // DielectricBsdf (src/surfaces/microfacet.rs:155-307)
+    V3<T> refraction_half(V3<T> wi, V3<T> wo, T e) const {
+        V3<T> h = -normalize(wo + wi * e);
+        if (h.z * wo.z < T(0)) h = -h;
+        return h;
+    }
+    V3<T> dielectric_eval(V3<T> wi, V3<T> wo) const {
+        T cos_wo = abs_cos_theta(wo), cos_wi = abs_cos_theta(wi);
+        if (cos_wo == T(0) || cos_wi == T(0)) return {};
+        T v;
+        if (same_hemisphere(wi, wo)) {
+            V3<T> h = normalize(wi + wo);
+            T f = fresnel_dielectric(std::fabs(dot(wi, h)), eta);
+            v = ((f * ggx_d(alpha, h)) * ggx_g2(alpha, wi, wo)) / ((T(4) * cos_wi) * cos_wo);
+        } else {
+            T e = wo.z > T(0) ? eta : T(1) / eta;
+            V3<T> h = refraction_half(wi, wo, e);
+            T woh = dot(wo, h), wih = dot(wi, h);
+            if (woh == T(0) || wih == T(0)) return {};
+            T f = T(1) - fresnel_dielectric(std::fabs(wih), eta);
+            T d = ggx_d(alpha, h), g = ggx_g2(alpha, wi, wo);
+            T sum = woh + e * wih;
+            T denom = sum * sum;  // powi(2)
+            if (denom == T(0)) return {};
+            T eta2 = e * e;
+            v = ((((f * d) * g) * eta2) * std::fabs(woh)) * std::fabs(wih) / ((cos_wi * cos_wo) * denom);
+        }
+        return V3<T>(v, v, v);
+    }
+    T dielectric_pdf(V3<T> wi, V3<T> wo) const {
+        if (abs_cos_theta(wo) == T(0) || abs_cos_theta(wi) == T(0)) return T(0);
+        if (same_hemisphere(wi, wo)) {
+            V3<T> h = normalize(wi + wo);
+            T whwi = std::fabs(dot(wi, h));
+            if (whwi == T(0)) return T(0);
+            T f = fresnel_dielectric(std::fabs(dot(wo, h)), eta);
+            return ((f * ggx_d(alpha, h)) * abs_cos_theta(h)) / (T(4) * whwi);
+        }
+        T e = wo.z > T(0) ? eta : T(1) / eta;
+        V3<T> h = refraction_half(wi, wo, e);
+        T woh = dot(wo, h), wih = dot(wi, h);
+        if (woh == T(0) || wih == T(0)) return T(0);
+        T sum = woh + e * wih;
+        T denom = sum * sum;
+        if (denom == T(0)) return T(0);
+        T f = T(1) - fresnel_dielectric(std::fabs(woh), eta);
+        return (((((f * ggx_d(alpha, h)) * abs_cos_theta(h)) * e) * e) * std::fabs(wih)) / denom;
+    }
 
     V3<T> eval(V3<T> wi, V3<T> wo) const {
+        if (kind == AR_MATERIAL_DIELECTRIC) return dielectric_eval(wi, wo);
         if (kind == AR_MATERIAL_LAMBERTIAN) {
             if (!same_hemisphere(wi, wo)) return {};
             return albedo * frac_1_pi<T>();
@@ -127,6 +205,7 @@ struct Material {
         return f * (d * g / ((T(4) * ci) * co));
     }
     T pdf(V3<T> wi, V3<T> wo) const {
+        if (kind == AR_MATERIAL_DIELECTRIC) return dielectric_pdf(wi, wo);
         if (kind == AR_MATERIAL_LAMBERTIAN) {
             if (!same_hemisphere(wi, wo)) return T(0);
             return abs_cos_theta(wi) * frac_1_pi<T>();
@@ -137,7 +216,7 @@ struct Material {
         if (whwi == T(0)) return T(0);
         return ggx_d(alpha, h) * abs_cos_theta(h) / (T(4) * whwi);
     }
-    BsdfSample<T> sample(V3<T> wo, T /*u_sel*/, V2<T> u) const {
+    BsdfSample<T> sample(V3<T> wo, T u_sel, V2<T> u) const {
         BsdfSample<T> s{};
         s.valid = false;
         if (kind == AR_MATERIAL_LAMBERTIAN) {
@@ -150,6 +229,17 @@ struct Material {
         }
         if (wo.z == T(0)) return s;
         V3<T> h = ggx_sample_wh(alpha, wo, u);
+        if (kind == AR_MATERIAL_DIELECTRIC && !(u_sel < fresnel_dielectric(std::fabs(dot(wo, h)), eta))) {
+            // refraction lobe (microfacet.rs:248-264)
+            T e = wo.z > T(0) ? T(1) / eta : eta;
+            V3<T> wi;
+            if (!refract(wo, h, e, wi)) return s;
+            if (same_hemisphere(wi, wo)) return s;
+            T p = pdf(wi, wo);
+            if (p == T(0)) return s;
+            s = {wi, p, eval(wi, wo), true};
+            return s;
+        }
         V3<T> wi = reflect(wo, h);
         if (!same_hemisphere(wi, wo)) return s;
         T p = pdf(wi, wo);
@@ -531,6 +621,7 @@ struct Scene {
             mm.f0 = V3<T>(T(m.f0[0]), T(m.f0[1]), T(m.f0[2]));
             float a = m.roughness < 1e-3f ? 1e-3f : (m.roughness > 1.0f ? 1.0f : m.roughness);
             mm.alpha = T(a);
+            mm.eta = T(m.eta);
         }
         lights.resize(d.num_lights);
         for (uint32_t i = 0; i < d.num_lights; ++i) {

@@ -172,3 +172,17 @@ def test_header_symbols_exported():
         assert hasattr(lb, name), name
     assert decls == set(_lib.SIGNATURES), decls ^ set(_lib.SIGNATURES)
     assert lb.ar_abi_version() == 1
+
+
+def test_oracle_dielectric_scene_is_finite_and_transmits():
+    # The glass Cornell box renders finite values, and the glass lets light
+    # through: pixels behind the glass sphere are not black.
+    sc, cam = S.cornell_box(1, glass=True)
+    osc = O.OracleScene(sc)
+    img = osc.render(cam, integrator_cfg(A.INTEGRATOR_PT, spp=32, max_depth=8, seed=3), 24, 24)
+    assert np.isfinite(img).all()
+    assert img.mean() > 0.05
+    # swapping the glass for an opaque black-free Lambertian changes the image
+    plain, _ = S.cornell_box(1)
+    other = O.OracleScene(plain).render(cam, integrator_cfg(A.INTEGRATOR_PT, spp=32, max_depth=8, seed=3), 24, 24)
+    assert np.abs(img - other).mean() > 1e-3

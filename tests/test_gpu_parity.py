@@ -254,3 +254,36 @@ def test_film_to_rgb8_matches_oracle(ctx, tm, wp):
     import torch
     dev = agentray.film_to_rgb8(ctx, torch.from_numpy(hdr).cuda(), tm, 2.2, 1.0, wp)
     np.testing.assert_array_equal(dev.cpu().numpy(), agentray.film_to_rgb8(ctx, hdr, tm, 2.2, 1.0, wp))
+
+
+# Same stream through glass: a ulp of difference in CUDA's cosf/sinf/sqrtf
+# versus the host's bends a refracted path onto other surfaces, and BDPT
+# connects every vertex of both subpaths, so fewer pixels agree exactly than
+# without glass (~0.90 vs 1.00 for BDPT; measured); the bias bar stays (mean
+# within 1.5%) and the independent-seed test below shows no bias.
+@pytest.mark.parametrize("kind,spp,frac", [(A.INTEGRATOR_PT, 16, 0.95), (A.INTEGRATOR_BDPT, 8, 0.85)])
+def test_dielectric_same_stream_matches_oracle(ctx, kind, spp, frac):
+    # DielectricBsdf (rough GGX glass): refraction, total internal reflection
+    # and the reference's face-forwarded frame (wo.z > 0, so eta is always the
+    # "entering" one), in PT and BDPT.
+    sc, cam = S.cornell_box(1, glass=True)
+    cfg = integrator_cfg(kind, spp=spp, max_depth=8, rr_depth=3, seed=6)
+    w = h = 48
+    gpu = _render_gpu(ctx, sc, cam, cfg, w, h)
+    ref = O.OracleScene(sc).render(cam, cfg, w, h, sampler=O.SAMPLER_COUNTER)
+    assert np.isfinite(gpu).all()
+    assert abs(gpu.mean() - ref.mean()) / ref.mean() < 1.5e-2
+    close = np.abs(gpu - ref) <= 1e-2 * np.maximum(1.0, np.abs(ref))
+    assert close.all(axis=2).mean() >= frac, close.all(axis=2).mean()
+
+
+@pytest.mark.parametrize("kind", [A.INTEGRATOR_PT, A.INTEGRATOR_BDPT])
+def test_dielectric_statistically_equal_to_independent_oracle(ctx, kind):
+    sc, cam = S.cornell_box(1, glass=True)
+    w = h = 32
+    osc = O.OracleScene(sc)
+    g = np.stack([_render_gpu(ctx, sc, cam, integrator_cfg(kind, spp=16, max_depth=8, seed=700 + k), w, h)
+                  for k in range(8)])
+    r = np.stack([osc.render(cam, integrator_cfg(kind, spp=16, max_depth=8, seed=800 + k), w, h,
+                             sampler=O.SAMPLER_COUNTER) for k in range(8)])
+    assert welch_fail_fraction(g, r) < 0.01

@@ -32,6 +32,8 @@ SIGNATURES = {
     "ar_trace_closest": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(A.RayBatch), C.c_void_p, C.c_void_p,
                                    C.c_uint32]),
     "ar_trace_any": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(A.RayBatch), C.c_void_p, C.c_uint32]),
+    "ar_render_samples": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(A.CameraDesc), C.POINTER(A.IntegratorCfg),
+                                    C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32]),
     "ar_render": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(A.CameraDesc), C.POINTER(A.IntegratorCfg),
                             C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32]),
     "ar_poisson_reconstruct": (C.c_int, [C.c_void_p, C.POINTER(A.IntegratorCfg), C.c_uint32, C.c_uint32,

@@ -867,7 +867,9 @@ BdJob make_bdpt_job(const ar_scene* sc, const CameraDev& cam, const ar_integrato
 void render_bdpt_film(ar_context* ctx, const ar_scene* sc, const CameraDev& cam, const ar_integrator_cfg& cfg,
                       uint32_t w, uint32_t h, void* film) {
     AR_REQUIRE(cfg.max_depth <= 62, AR_ERR_INVALID_ARGUMENT, "max_depth must be <= 62");
-    const uint64_t total = uint64_t(w) * h * cfg.spp;
+    const uint64_t npix = uint64_t(w) * h;
+    const uint32_t s0 = ctx->range_end ? ctx->range_begin : 0u, s1 = ctx->range_end ? ctx->range_end : cfg.spp;
+    const uint64_t first = npix * s0, total = npix * (s1 - s0);
     const size_t budget = ctx->bdpt_budget;
     const size_t per = bdpt_batch_bytes(cfg.max_depth, 1024) / 1024 + 1;
     const uint32_t batch = uint32_t(std::max<uint64_t>(1024, std::min<uint64_t>(total, budget / per)));
@@ -885,7 +887,7 @@ void render_bdpt_film(ar_context* ctx, const ar_scene* sc, const CameraDev& cam,
     uint64_t batches = 0;
     for (uint64_t begin = 0; begin < total; begin += cap, ++batches) {
         const uint32_t n = uint32_t(std::min<uint64_t>(cap, total - begin));
-        bdpt_run_batch(ctx->bdpt, jobs, {BdSegment{0, 0, n, 0, begin}});
+        bdpt_run_batch(ctx->bdpt, jobs, {BdSegment{0, 0, n, 0, first + begin}});
     }
     AR_CUDA(cudaMemcpyAsync(ctx->stats_h, ctx->stats_d.ptr, 8 * sizeof(uint64_t), cudaMemcpyDeviceToHost,
                             ctx->stream));

@@ -206,6 +206,28 @@ int ar_render(ar_context* ctx, const ar_scene* scene, const ar_camera_desc* came
     });
 }
 
+int ar_render_samples(ar_context* ctx, const ar_scene* scene, const ar_camera_desc* camera,
+                      const ar_integrator_cfg* cfg, uint32_t width, uint32_t height, uint32_t sample_begin,
+                      uint32_t sample_end, float* out_rgb, uint32_t out_on_device) {
+    return guarded([&] {
+        AR_REQUIRE(ctx && scene && camera && cfg && out_rgb, AR_ERR_INVALID_ARGUMENT, "null argument");
+        AR_REQUIRE(width > 0 && height > 0, AR_ERR_INVALID_ARGUMENT, "empty image");
+        AR_REQUIRE(cfg->spp > 0, AR_ERR_INVALID_ARGUMENT, "spp must be positive");
+        AR_REQUIRE(sample_begin < sample_end && sample_end <= cfg->spp, AR_ERR_INVALID_ARGUMENT,
+                   "sample range must be a non-empty part of [0, spp)");
+        AR_REQUIRE(cfg->integrator != AR_INTEGRATOR_GDPT, AR_ERR_INVALID_ARGUMENT,
+                   "GDPT reconstructs from all samples: shard PT or BDPT");
+        AR_CUDA(cudaSetDevice(ctx->device));
+        struct Reset {
+            ar_context* c;
+            ~Reset() { c->range_begin = c->range_end = 0; }
+        } reset{ctx};
+        ctx->range_begin = sample_begin;
+        ctx->range_end = sample_end;
+        render(ctx, scene, *camera, *cfg, width, height, out_rgb, out_on_device != 0);
+    });
+}
+
 int ar_poisson_reconstruct(ar_context* ctx, const ar_integrator_cfg* cfg, uint32_t width, uint32_t height,
                            const float* primal, const float* grad_x, const float* grad_y, float* out,
                            uint32_t on_device, double* rel_residual) {

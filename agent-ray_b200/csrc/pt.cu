@@ -562,9 +562,11 @@ void render_pt_films(ar_context* ctx, const ar_scene* sc, const CameraDev& cam, 
     J.seed = cfg.seed;
     J.inv_spp = 1.0f / float(cfg.spp);
     for (uint32_t f = 0; f < roles; ++f) J.film[f] = static_cast<char*>(films) + f * film_bytes;
-    J.total_samples = uint64_t(w) * h * cfg.spp;
-    J.total_paths = J.total_samples * roles;
-    J.next_sample = 0;
+    const uint64_t npix = uint64_t(w) * h;
+    const uint32_t s0 = ctx->range_end ? ctx->range_begin : 0u, s1 = ctx->range_end ? ctx->range_end : cfg.spp;
+    J.total_samples = npix * s1;  // sample g of the job is pixel g % npix, sample g / npix
+    J.total_paths = npix * (s1 - s0) * roles;
+    J.next_sample = npix * s0;
     J.done_paths = 0;
     const uint32_t slot = 0;
     unsigned long long before[3];
@@ -599,7 +601,7 @@ void render_pt_films(ar_context* ctx, const ar_scene* sc, const CameraDev& cam, 
     engine_remove_job(e, slot);
     unsigned long long after[3];
     AR_CUDA(cudaMemcpy(after, e->E.stats, sizeof(after), cudaMemcpyDeviceToHost));
-    ctx->last_stats.path_samples = J.total_samples;
+    ctx->last_stats.path_samples = npix * (s1 - s0);
     ctx->last_stats.paths = after[0] - before[0];
     ctx->last_stats.extend_rays = after[1] - before[1];
     ctx->last_stats.shadow_rays = after[2] - before[2];

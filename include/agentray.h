@@ -294,6 +294,16 @@ int ar_render(ar_context* ctx, const ar_scene* scene, const ar_camera_desc* came
               const ar_integrator_cfg* cfg, uint32_t width, uint32_t height,
               float* out_rgb, uint32_t out_on_device);
 
+/* Renders only samples [sample_begin, sample_end) of every pixel, each weighted
+ * by 1/spp, so the images of disjoint ranges sum to the ar_render image (with
+ * the same seed): multi-GPU sample sharding, each rank rendering its range
+ * before a film sum (e.g. an NCCL all-reduce).  PT and BDPT only (GDPT solves
+ * its Poisson system after all samples).  No reference counterpart: the
+ * reference renders all samples in one process. */
+int ar_render_samples(ar_context* ctx, const ar_scene* scene, const ar_camera_desc* camera,
+                      const ar_integrator_cfg* cfg, uint32_t width, uint32_t height, uint32_t sample_begin,
+                      uint32_t sample_end, float* out_rgb, uint32_t out_on_device);
+
 /* ---- film output (src/film.rs:136-302) ---- */
 
 enum ar_tone_mapper {

@@ -287,3 +287,23 @@ def test_dielectric_statistically_equal_to_independent_oracle(ctx, kind):
     r = np.stack([osc.render(cam, integrator_cfg(kind, spp=16, max_depth=8, seed=800 + k), w, h,
                              sampler=O.SAMPLER_COUNTER) for k in range(8)])
     assert welch_fail_fraction(g, r) < 0.01
+
+
+@pytest.mark.parametrize("kind", [A.INTEGRATOR_PT, A.INTEGRATOR_BDPT])
+def test_sample_range_shards_sum_to_full_render(ctx, kind):
+    # Multi-GPU sharding on one GPU: disjoint sample ranges rendered apart
+    # (ar_render_samples) sum to the one-call render (FP64 films).
+    from agentray import distributed as D
+    sc, cam = S.cornell_box(1)
+    g = agentray.Scene(ctx, sc)
+    cls, cfg_cls = ((agentray.PathTracer, agentray.PathTracerConfig) if kind == A.INTEGRATOR_PT else
+                    (agentray.BidirectionalPathTracer, agentray.BdptConfig))
+    integ = cls(cfg_cls(spp=10, max_depth=6, seed=12, film_precision=A.FILM_F64))
+    w, h = 40, 32
+    full = integ.render(g, cam, w, h).rgb.astype(np.float64)
+    parts = [D.render_shard(integ, g, cam, w, h, *D.shard_range(10, r, 3), np.zeros(w * h * 3, np.float32))
+             for r in range(3)]
+    total = np.sum([p.astype(np.float64) for p in parts], axis=0).reshape(h, w, 3)
+    np.testing.assert_allclose(total, full, rtol=1e-5, atol=1e-6)
+    with pytest.raises(agentray.AgentRayError):
+        D.render_shard(integ, g, cam, w, h, 5, 11, np.zeros(w * h * 3, np.float32))

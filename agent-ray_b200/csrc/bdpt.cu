@@ -52,6 +52,9 @@ struct BdParams {
     float4* va;  // p.xyz, pdf_fwd
     float4* vb;  // n.xyz, pdf_rev
     float4* vc;  // thr.xyz, info (type << 30 | delta << 29 | index)
+    float4* sva; // the three vertex arrays permuted into the (S, T)-sorted sample
+    float4* svb; // order, so the connection kernel's warps read them coalesced
+    float4* svc;
     uint8_t* nv; // [sub * nsamples + si]
     float4* thr; // per subpath q = 2 si + sub: thr.xyz, previous directional pdf
     uint32_t* dim;
@@ -640,9 +643,30 @@ __global__ void __launch_bounds__(256) k_bd_scatter(BdParams P) {
     if (live) P.order[base[key] + rank] = si;
 }
 
+// Copies every sample's vertices to its sorted position oi (reads scattered,
+// writes coalesced), so k_bd_connect, whose thread oi handles sample
+// order[oi], reads vertex k of 32 consecutive samples as one contiguous block.
+__global__ void __launch_bounds__(256) k_bd_permute(BdParams P) {
+    for (uint32_t oi = blockIdx.x * blockDim.x + threadIdx.x; oi < P.nsamples; oi += gridDim.x * blockDim.x) {
+        const uint32_t si = P.order[oi];
+        for (uint32_t sub = 0; sub < 2; ++sub) {
+            const uint32_t n = P.nv[sub * P.nsamples + si];
+            for (uint32_t k = 0; k < n; ++k) {
+                const size_t from = vidx(P, sub, k, si), to = vidx(P, sub, k, oi);
+                P.sva[to] = P.va[from];
+                P.svb[to] = P.vb[from];
+                P.svc[to] = P.vc[from];
+            }
+        }
+    }
+}
+
 // One thread per sample: the MIS prefix sums are built once, then the
 // strategies run camera-vertex-major so each z's frame is computed once.
 __global__ void __launch_bounds__(128) k_bd_connect(BdParams P) {
+    // P.va/vb/vc are the sorted copies here (see bdpt_run_batch): vertex
+    // records of sample order[oi] are read at index oi; the per-sample arrays
+    // (job, lengths, global index) stay indexed by the sample itself.
     for (uint32_t oi = blockIdx.x * blockDim.x + threadIdx.x; oi < P.nsamples; oi += gridDim.x * blockDim.x) {
         const uint32_t si = P.order[oi];
         const uint32_t job = P.sjob[si];
@@ -651,14 +675,14 @@ __global__ void __launch_bounds__(128) k_bd_connect(BdParams P) {
         const uint32_t pix = uint32_t(P.sindex[si] % (J.width * J.height));
         const uint32_t limit = J.max_depth + 2;
         MisCache mc;
-        build_mis_cache(P, J, si, S, T, mc);
+        build_mis_cache(P, J, oi, S, T, mc);
         bool lpt = false;
-        if (T >= 1) lpt = J.sc.lights[load_vtx(P, 1, 0, si).index].kind == AR_LIGHT_POINT;
+        if (T >= 1) lpt = J.sc.lights[load_vtx(P, 1, 0, oi).index].kind == AR_LIGHT_POINT;
         if (S >= 1)
-            for (uint32_t t = 2; t <= T && 1 + t <= limit; ++t) connect_s1(P, J, job, si, S, T, mc, lpt, t);
+            for (uint32_t t = 2; t <= T && 1 + t <= limit; ++t) connect_s1(P, J, job, oi, S, T, mc, lpt, t);
         for (uint32_t s = 2; s <= S; ++s) {
-            const CamSide cs = cam_side(P, J, si, s);
-            for (uint32_t t = 0; t <= T && s + t <= limit; ++t) connect_general(P, J, job, si, S, T, mc, lpt, cs, s, t, pix);
+            const CamSide cs = cam_side(P, J, oi, s);
+            for (uint32_t t = 0; t <= T && s + t <= limit; ++t) connect_general(P, J, job, oi, S, T, mc, lpt, cs, s, t, pix);
         }
     }
 }
@@ -723,7 +747,7 @@ struct BdptBatcher {
 
 size_t bdpt_batch_bytes(uint32_t max_depth, uint32_t batch) {
     const size_t maxv = max_depth + 1;
-    const size_t per_sample = 2 * maxv * 48 + 2 + 2 * (16 + 4) + 2 * 2 * (32 + 4) + 2 * 20 + 4 + 8 +
+    const size_t per_sample = 2 * 2 * maxv * 48 + 2 + 2 * (16 + 4) + 2 * 2 * (32 + 4) + 2 * 20 + 4 + 8 +
                               size_t(max_pairs_for(max_depth)) * 52 + 4;
     return per_sample * batch + 64 * 1024;
 }
@@ -749,6 +773,9 @@ BdptBatcher* bdpt_create(ar_context* ctx, uint32_t max_depth_cap, uint32_t batch
     P.va = carve<float4>(cur, nvtx);
     P.vb = carve<float4>(cur, nvtx);
     P.vc = carve<float4>(cur, nvtx);
+    P.sva = carve<float4>(cur, nvtx);
+    P.svb = carve<float4>(cur, nvtx);
+    P.svc = carve<float4>(cur, nvtx);
     P.nv = carve<uint8_t>(cur, 2 * size_t(batch));
     P.thr = carve<float4>(cur, 2 * size_t(batch));
     P.dim = carve<uint32_t>(cur, 2 * size_t(batch));
@@ -832,9 +859,17 @@ void bdpt_run_batch(BdptBatcher* b, const std::vector<BdJob>& jobs, const std::v
         k_bd_scatter<<<g, 256, 0, ctx->stream>>>(P);
     }
     {
+        KernelScope ks(ctx->prof, ctx->stream, "bdpt_permute");
+        k_bd_permute<<<std::max(1, int(std::min<uint64_t>((nsamples + 255) / 256, wide))), 256, 0, ctx->stream>>>(P);
+    }
+    {
         KernelScope ks(ctx->prof, ctx->stream, "bdpt_connect");
+        BdParams Pc = P;
+        Pc.va = P.sva;
+        Pc.vb = P.svb;
+        Pc.vc = P.svc;
         k_bd_connect<<<std::max(1, int(std::min<uint64_t>((nsamples + 127) / 128, ctx->num_sms * 16))), 128, 0,
-                       ctx->stream>>>(P);
+                       ctx->stream>>>(Pc);
     }
     {
         KernelScope ks(ctx->prof, ctx->stream, "bdpt_shadow");

@@ -137,7 +137,7 @@ struct ar_context {
     // launch shapes (ar_tuning)
     uint32_t trav_blocks_per_sm = 8;       // persistent traversal grid, blocks per SM
     uint32_t shade_block = 256;            // threads per block of the shading stage
-    size_t bdpt_budget = size_t(3) << 30;  // HBM for one plain-path BDPT batch
+    size_t bdpt_budget = size_t(12) << 30;  // HBM for one plain-path BDPT batch
     // samples [range_begin, range_end) of each pixel for the next render
     // (ar_render_samples); range_end == 0 renders all spp samples
     uint32_t range_begin = 0, range_end = 0;

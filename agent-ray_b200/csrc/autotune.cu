@@ -34,7 +34,7 @@ void set_tuning(ar_context* ctx, const ar_tuning& t) {
     const uint32_t cap = t.path_capacity ? t.path_capacity : (1u << 21);
     const uint32_t tb = t.traversal_blocks_per_sm ? t.traversal_blocks_per_sm : 8u;
     const uint32_t sb = t.shade_block ? t.shade_block : 256u;
-    const uint32_t mib = t.bdpt_batch_mib ? t.bdpt_batch_mib : 3072u;
+    const uint32_t mib = t.bdpt_batch_mib ? t.bdpt_batch_mib : 12288u;
     AR_REQUIRE(cap >= 4096 && cap <= (1u << 26), AR_ERR_INVALID_ARGUMENT, "path_capacity must be in [4096, 2^26]");
     AR_REQUIRE(tb >= 1 && tb <= 8, AR_ERR_INVALID_ARGUMENT, "traversal_blocks_per_sm must be 1..8");
     AR_REQUIRE(sb == 64 || sb == 128 || sb == 256, AR_ERR_INVALID_ARGUMENT, "shade_block must be 64, 128 or 256");
@@ -169,7 +169,7 @@ void autotune(ar_context* ctx, ar_scene* sc, const ar_camera_desc& cam, const ar
     sweep(&ar_tuning::traversal_blocks_per_sm, {8u, 6u, 4u});
     sweep(&ar_tuning::shade_block, {256u, 128u, 64u});
     if (o.integrator == AR_INTEGRATOR_BDPT)
-        sweep(&ar_tuning::bdpt_batch_mib, {768u, 1536u, 3072u, 6144u});
+        sweep(&ar_tuning::bdpt_batch_mib, {3072u, 6144u, 12288u, 24576u});
     else
         sweep(&ar_tuning::path_capacity, {1u << 19, 1u << 20, 1u << 21, 1u << 22});
     r.tuning = best;

@@ -133,7 +133,7 @@ struct ar_context {
     ar_render_stats last_stats{};
     bool stats_pending = false;
     ar::PathEngine* engine = nullptr;  // streaming wavefront engine for ar_render
-    uint32_t engine_capacity = 1u << 21;
+    uint32_t engine_capacity = 1u << 22;
     // launch shapes (ar_tuning)
     uint32_t trav_blocks_per_sm = 8;       // persistent traversal grid, blocks per SM
     uint32_t shade_block = 256;            // threads per block of the shading stage

@@ -31,7 +31,7 @@ ar_tuning get_tuning(const ar_context* ctx) {
 }
 
 void set_tuning(ar_context* ctx, const ar_tuning& t) {
-    const uint32_t cap = t.path_capacity ? t.path_capacity : (1u << 21);
+    const uint32_t cap = t.path_capacity ? t.path_capacity : (1u << 22);
     const uint32_t tb = t.traversal_blocks_per_sm ? t.traversal_blocks_per_sm : 8u;
     const uint32_t sb = t.shade_block ? t.shade_block : 256u;
     const uint32_t mib = t.bdpt_batch_mib ? t.bdpt_batch_mib : 12288u;
@@ -171,7 +171,7 @@ void autotune(ar_context* ctx, ar_scene* sc, const ar_camera_desc& cam, const ar
     if (o.integrator == AR_INTEGRATOR_BDPT)
         sweep(&ar_tuning::bdpt_batch_mib, {3072u, 6144u, 12288u, 24576u});
     else
-        sweep(&ar_tuning::path_capacity, {1u << 19, 1u << 20, 1u << 21, 1u << 22});
+        sweep(&ar_tuning::path_capacity, {1u << 20, 1u << 21, 1u << 22, 1u << 23});
     r.tuning = best;
     r.accel = best_accel;
     r.best_ms = best_ms;

@@ -436,7 +436,7 @@ int ar_server_create(ar_context* ctx, const ar_server_opts* o, ar_server** out) 
         S.device = ctx->device;
         if (o) S.opts = *o;
         if (!S.opts.film_budget_bytes) S.opts.film_budget_bytes = 8ull << 30;
-        if (!S.opts.path_capacity) S.opts.path_capacity = 1u << 21;
+        if (!S.opts.path_capacity) S.opts.path_capacity = 1u << 22;
         if (!S.opts.bdpt_batch_samples) S.opts.bdpt_batch_samples = 1u << 20;
         if (!S.opts.bdpt_max_depth) S.opts.bdpt_max_depth = 10;
         if (!S.opts.max_active_jobs || S.opts.max_active_jobs > kMaxActiveJobs) S.opts.max_active_jobs = kMaxActiveJobs;

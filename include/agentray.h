@@ -236,7 +236,7 @@ int ar_context_synchronize(ar_context* ctx);
 /* Launch and queue parameters of a context (the autotuner's search space).
  * No reference counterpart: the reference's CPU integrators have no such knobs. */
 typedef struct ar_tuning {
-    uint32_t path_capacity;          /* PT/GDPT engine path slots (queue capacity; 0: 2^21) */
+    uint32_t path_capacity;          /* PT/GDPT engine path slots (queue capacity; 0: 2^22) */
     uint32_t traversal_blocks_per_sm;/* persistent traversal grid, 128-thread blocks per SM, 1..8 (0: 8) */
     uint32_t shade_block;            /* threads per block of the shading stage: 64, 128 or 256 (0: 256) */
     uint32_t bdpt_batch_mib;         /* HBM for one BDPT batch of ar_render, MiB (0: 12288) */

@@ -800,6 +800,8 @@ def main():
     ap.add_argument("--served-jobs", dest="served_jobs", type=int, default=160)
     ap.add_argument("--path-capacity", dest="path_capacity", type=int, default=1 << 22)
     ap.add_argument("--bdpt-batch", dest="bdpt_batch", type=int, default=1 << 21)
+    ap.add_argument("--bdpt-batch-mib", dest="bdpt_batch_mib", type=int, default=0,
+                    help="HBM per plain-path BDPT batch (0: the library default)")
     ap.add_argument("--cpu-samples", dest="cpu_samples", type=int, default=4_000_000)
     args = ap.parse_args()
     rank, local, world = dist_env()
@@ -822,6 +824,8 @@ def main():
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
+    if args.bdpt_batch_mib:
+        ctx.set_tuning(bdpt_batch_mib=args.bdpt_batch_mib)
 
     def barrier():
         if dist is not None:

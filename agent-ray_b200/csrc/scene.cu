@@ -45,7 +45,6 @@ void upload(DevBuf& d, const std::vector<T>& h) {
 struct V3f {
     float x, y, z;
 };
-inline V3f sub(V3f a, V3f b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
 inline V3f mulf(V3f a, float s) { return {a.x * s, a.y * s, a.z * s}; }
 inline V3f addv(V3f a, V3f b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
 inline float dotf(V3f a, V3f b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }

@@ -43,8 +43,8 @@ f32 = C.c_float
 
 class MeshDesc(C.Structure):
     _fields_ = [("positions", C.c_void_p), ("normals", C.c_void_p), ("indices", C.c_void_p),
-                ("material_slots", C.c_void_p), ("num_vertices", u32), ("num_triangles", u32),
-                ("num_material_slots", u32), ("_pad", u32)]
+                ("material_slots", C.c_void_p), ("tex_coords", C.c_void_p), ("num_vertices", u32),
+                ("num_triangles", u32), ("num_material_slots", u32), ("_pad", u32)]
 
 
 class ObjectDesc(C.Structure):
@@ -54,7 +54,11 @@ class ObjectDesc(C.Structure):
 
 class MaterialDesc(C.Structure):
     _fields_ = [("kind", u32), ("emitter_light", C.c_int32), ("albedo", f32 * 3), ("f0", f32 * 3),
-                ("roughness", f32), ("eta", f32)]
+                ("roughness", f32), ("eta", f32), ("albedo_texture", C.c_int32), ("_pad", u32)]
+
+
+class TextureDesc(C.Structure):
+    _fields_ = [("rgb8", C.c_void_p), ("width", u32), ("height", u32)]
 
 
 class LightDesc(C.Structure):
@@ -64,8 +68,8 @@ class LightDesc(C.Structure):
 
 class SceneDesc(C.Structure):
     _fields_ = [("meshes", C.c_void_p), ("objects", C.c_void_p), ("materials", C.c_void_p),
-                ("lights", C.c_void_p), ("num_meshes", u32), ("num_objects", u32), ("num_materials", u32),
-                ("num_lights", u32), ("light_distribution", u32), ("_pad", u32)]
+                ("lights", C.c_void_p), ("textures", C.c_void_p), ("num_meshes", u32), ("num_objects", u32),
+                ("num_materials", u32), ("num_lights", u32), ("light_distribution", u32), ("num_textures", u32)]
 
 
 class CameraDesc(C.Structure):
@@ -117,7 +121,10 @@ class SceneStats(C.Structure):
 
 assert C.sizeof(IntegratorCfg) == 64
 assert C.sizeof(ObjectDesc) == 152
-assert C.sizeof(MaterialDesc) == 40
+assert C.sizeof(MaterialDesc) == 48
+assert C.sizeof(MeshDesc) == 56
+assert C.sizeof(TextureDesc) == 16
+assert C.sizeof(SceneDesc) == 64
 assert C.sizeof(LightDesc) == 56
 
 

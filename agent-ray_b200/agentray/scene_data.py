@@ -17,6 +17,7 @@ class Mesh:
     indices: np.ndarray                   # (T, 3) uint32
     normals: Optional[np.ndarray] = None  # (V, 3) float32
     material_slots: Optional[np.ndarray] = None  # (1,) or (T,) uint32
+    tex_coords: Optional[np.ndarray] = None  # (V, 2) float32
 
     @property
     def num_triangles(self):
@@ -31,6 +32,7 @@ class Material:
     roughness: float = 0.3
     emitter_light: int = -1
     eta: float = 1.5  # dielectric interior index of refraction
+    albedo_texture: int = -1  # Lambertian: index into SceneData.textures
 
 
 @dataclass
@@ -82,6 +84,7 @@ class SceneData:
         self.objects: List[Object] = []
         self.materials: List[Material] = []
         self.lights: List[Light] = []
+        self.textures: List[np.ndarray] = []  # (H, W, 3) uint8 sRGB images (ImageTexture)
         self.light_distribution = light_distribution
 
     def add_mesh(self, mesh: Mesh) -> int:
@@ -95,6 +98,14 @@ class SceneData:
     def add_object(self, obj: Object) -> int:
         self.objects.append(obj)
         return len(self.objects) - 1
+
+    def add_texture(self, rgb8: np.ndarray) -> int:
+        """Adds an 8-bit sRGB image (H, W, 3), row 0 at the top (ImageTexture::load)."""
+        img = np.ascontiguousarray(rgb8, dtype=np.uint8)
+        if img.ndim != 3 or img.shape[2] != 3 or img.shape[0] == 0 or img.shape[1] == 0:
+            raise ValueError("texture must be a non-empty (H, W, 3) uint8 image")
+        self.textures.append(img)
+        return len(self.textures) - 1
 
     def add_light(self, light: Light) -> int:
         self.lights.append(light)
@@ -125,6 +136,10 @@ class SceneData:
                 nrm = np.ascontiguousarray(m.normals, dtype=np.float32)
                 keep.append(nrm)
                 meshes[i].normals = nrm.ctypes.data
+            if m.tex_coords is not None:
+                uv = np.ascontiguousarray(m.tex_coords, dtype=np.float32)
+                keep.append(uv)
+                meshes[i].tex_coords = uv.ctypes.data
         objs = (A.ObjectDesc * max(1, len(self.objects)))()
         for i, o in enumerate(self.objects):
             objs[i].transform[:] = _colmajor(o.transform).tolist()
@@ -144,6 +159,7 @@ class SceneData:
             mats_d[i].f0[:] = [float(x) for x in m.f0]
             mats_d[i].roughness = float(m.roughness)
             mats_d[i].eta = float(m.eta)
+            mats_d[i].albedo_texture = int(m.albedo_texture)
         lights_d = (A.LightDesc * max(1, len(self.lights)))()
         for i, l in enumerate(self.lights):
             lights_d[i].kind = l.kind
@@ -151,12 +167,18 @@ class SceneData:
             lights_d[i].intensity[:] = [float(x) for x in l.intensity]
             lights_d[i].edge1[:] = [float(x) for x in l.edge1]
             lights_d[i].edge2[:] = [float(x) for x in l.edge2]
-        keep += [meshes, objs, mats_d, lights_d]
+        texs_d = (A.TextureDesc * max(1, len(self.textures)))()
+        for i, t in enumerate(self.textures):
+            texs_d[i].rgb8 = t.ctypes.data
+            texs_d[i].height, texs_d[i].width = int(t.shape[0]), int(t.shape[1])
+        keep += [meshes, objs, mats_d, lights_d, texs_d]
         d = A.SceneDesc()
         d.meshes = C.addressof(meshes)
         d.objects = C.addressof(objs)
         d.materials = C.addressof(mats_d)
         d.lights = C.addressof(lights_d)
+        d.textures = C.addressof(texs_d)
+        d.num_textures = len(self.textures)
         d.num_meshes = len(self.meshes)
         d.num_objects = len(self.objects)
         d.num_materials = len(self.materials)

@@ -99,9 +99,19 @@ def add_quad_light(sc, corner, e1, e2, radiance, visible=True):
 
 
 # ------------------------------------------------------------------ scenes --
-def cornell_box(seed=1, light_radiance=15.0, point_light=False, glass=False):
+def checker_texture(n=16, cells=4, seed=0):
+    """A seeded n x n 8-bit sRGB image: a checkerboard of random colours."""
+    rng = np.random.default_rng(seed)
+    cols = rng.integers(0, 256, (cells * cells, 3), dtype=np.uint8)
+    y, x = np.mgrid[0:n, 0:n]
+    cell = (y * cells // n) * cells + (x * cells // n)
+    return cols[cell]
+
+
+def cornell_box(seed=1, light_radiance=15.0, point_light=False, glass=False, textured=False):
     """Config-1 Cornell box: 5 walls (10 tris) + 2 rotated boxes (24 tris) and a
-    0.25 x 0.25 quad light of radiance 15 just below the ceiling.  glass=True
+    0.25 x 0.25 quad light of radiance 15 just below the ceiling.  textured=True
+    gives the floor and back wall checker ImageTextures.  glass=True
     makes the tall box a rough dielectric (eta 1.5, alpha 0.2) and adds a
     dielectric icosphere (eta 1.33, alpha 0.05)."""
     rng = np.random.default_rng(seed)
@@ -111,9 +121,17 @@ def cornell_box(seed=1, light_radiance=15.0, point_light=False, glass=False):
              ((0, 0, 0), (1, 0, 0), (0, 1, 0)),   # back
              ((0, 0, 0), (0, 1, 0), (0, 0, 1)),   # left
              ((1, 0, 0), (0, 0, 1), (0, 1, 0))]   # right
-    for c, e1, e2 in walls:
-        m = sc.add_mesh(quad_mesh(c, e1, e2))
+    for k, (c, e1, e2) in enumerate(walls):
+        mesh = quad_mesh(c, e1, e2)
         mat = sc.add_material(Material(A.MATERIAL_LAMBERTIAN, albedo=tuple(rng.uniform(0.2, 0.8, 3))))
+        if textured and k in (0, 2):
+            # floor and back wall: checker ImageTextures, uv repeating past [0, 1)
+            # and (back wall) negative, to exercise the repeat wrap
+            mesh.tex_coords = (np.array([[0, 0], [3, 0], [3, 3], [0, 3]], np.float32) if k == 0 else
+                               np.array([[-1.25, -0.5], [0.75, -0.5], [0.75, 1.5], [-1.25, 1.5]], np.float32))
+            tex = sc.add_texture(checker_texture(16 if k == 0 else 7, 4, seed=10 + k))
+            mat = sc.add_material(Material(A.MATERIAL_LAMBERTIAN, albedo_texture=tex))
+        m = sc.add_mesh(mesh)
         sc.add_object(Object(m, [mat]))
     cube = sc.add_mesh(unit_cube_mesh())
     for k, ((tx, ty, tz), deg, (sx, sy, sz)) in enumerate([((0.33, 0.3, 0.35), 15.0, (0.3, 0.6, 0.3)),

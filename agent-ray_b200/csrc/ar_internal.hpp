@@ -159,7 +159,7 @@ struct ar_scene {
     std::vector<float> light_power_weights;
     // device data
     ar::DevBuf nodes, tris, instances, objects_d, meshes_d, indices, normals, slots, mat_table, materials, lights,
-        light_cdf, light_pmf;
+        light_cdf, light_pmf, texcoords, texels, textures;
     ar::DevScene view{};
     ar_scene_stats stats{};
     ar_accel_opts accel{};  // options of the last build

@@ -7,6 +7,7 @@
 //   Lambertian                   src/surfaces/lambertian.rs:35-64
 //   ConductorBsdf (GGX)          src/surfaces/microfacet.rs:14-152
 //   DielectricBsdf (GGX glass)   src/surfaces/microfacet.rs:155-307, src/surfaces.rs:86-123
+//   ImageTexture                 src/texture.rs:65-151
 //   PointLight                   src/lights/point.rs:48-100
 //   Uniform/PowerLightDistribution src/lights.rs:136-235
 //   PinholeCamera                src/cameras.rs:146-248
@@ -40,6 +41,7 @@ struct Shade {
     Onb onb;
     uint32_t mat;
     uint32_t prim;
+    float tu, tv;  // tex_uv (SceneObject::tex_uv, src/scene.rs:54-66)
 };
 
 // Scene::intersect post-processing: world shading normal (interpolated vertex
@@ -68,6 +70,16 @@ __device__ __forceinline__ Shade make_shade(const DevScene& sc, f3 ro, f3 rd, fl
     s.n = n;
     s.onb = onb_from_normal(n);
     s.p = ro + rd * t;
+    if (mr.uv_offset != kInvalid) {  // tex_coords[i0] * w + tex_coords[i1] * u + tex_coords[i2] * v
+        const uint32_t* ix = sc.indices + mr.idx_offset + 3 * tr.prim;
+        const float* tc = sc.texcoords + 2 * size_t(mr.uv_offset);
+        const float w = (1.0f - u) - v;
+        s.tu = (tc[2 * ix[0]] * w + tc[2 * ix[1]] * u) + tc[2 * ix[2]] * v;
+        s.tv = (tc[2 * ix[0] + 1] * w + tc[2 * ix[1] + 1] * u) + tc[2 * ix[2] + 1] * v;
+    } else {
+        s.tu = u;
+        s.tv = v;
+    }
     const uint32_t si = mr.num_slots == 1 ? sc.material_slots[mr.slot_offset]
                                           : sc.material_slots[mr.slot_offset + tr.prim];
     const uint32_t k = min(si, ob.num_mats - 1);
@@ -110,6 +122,32 @@ struct MatView {
     float albedo[3], f0[3];
     float alpha, eta;
 };
+// ImageTexture::sample (src/texture.rs:97-136): repeat wrap, bilinear.
+__device__ __forceinline__ float wrap01(float x) {  // x.fract().rem_euclid(1.0)
+    const float f = x - truncf(x);
+    const float r = fmodf(f, 1.0f);
+    return r < 0.f ? r + 1.0f : r;
+}
+__device__ __forceinline__ f3 texel(const DevScene& sc, const TextureRecord& t, int32_t x, int32_t y) {
+    int32_t xm = x % int32_t(t.width), ym = y % int32_t(t.height);
+    if (xm < 0) xm += int32_t(t.width);
+    if (ym < 0) ym += int32_t(t.height);
+    const float4 c = __ldg(sc.texels + t.offset + uint32_t(ym) * t.width + uint32_t(xm));
+    return mk(c.x, c.y, c.z);
+}
+__device__ __forceinline__ f3 texture_sample(const DevScene& sc, uint32_t ti, float tu, float tv) {
+    const TextureRecord t = sc.textures[ti];
+    const float u = wrap01(tu) * float(t.width) - 0.5f;
+    const float v = wrap01(tv) * float(t.height) - 0.5f;
+    const float fu = floorf(u), fv = floorf(v);
+    const int32_t x0 = int32_t(fu), y0 = int32_t(fv);
+    const float tx = u - fu, ty = v - fv;
+    const f3 c00 = texel(sc, t, x0, y0), c10 = texel(sc, t, x0 + 1, y0), c01 = texel(sc, t, x0, y0 + 1),
+             c11 = texel(sc, t, x0 + 1, y0 + 1);
+    return ((c00 * ((1.0f - tx) * (1.0f - ty)) + c10 * (tx * (1.0f - ty))) + c01 * ((1.0f - tx) * ty)) +
+           c11 * (tx * ty);
+}
+
 __device__ __forceinline__ MatView load_mat(const DevScene& sc, uint32_t m) {
     const MaterialRecord& r = sc.materials[m];
     MatView v;
@@ -118,6 +156,20 @@ __device__ __forceinline__ MatView load_mat(const DevScene& sc, uint32_t m) {
     for (int k = 0; k < 3; ++k) { v.albedo[k] = r.albedo[k]; v.f0[k] = r.f0[k]; }
     v.alpha = r.alpha;
     v.eta = r.eta;
+    return v;
+}
+
+// The material at a shading point: a textured Lambertian's albedo is its
+// ImageTexture sampled at tex_uv (Lambertian::eval, lambertian.rs:35-41).
+__device__ __forceinline__ MatView load_mat_at(const DevScene& sc, uint32_t m, float tu, float tv) {
+    MatView v = load_mat(sc, m);
+    const int32_t ti = sc.materials[m].tex;
+    if (ti >= 0) {
+        const f3 a = texture_sample(sc, uint32_t(ti), tu, tv);
+        v.albedo[0] = a.x;
+        v.albedo[1] = a.y;
+        v.albedo[2] = a.z;
+    }
     return v;
 }
 

@@ -68,6 +68,7 @@ struct alignas(16) MeshRecord {
     uint32_t nrm_offset;   // into normals (3 floats per vertex), 0xFFFFFFFF when absent
     uint32_t slot_offset;  // into material_slots
     uint32_t num_slots;
+    uint32_t uv_offset;    // into texcoords (2 floats per vertex), 0xFFFFFFFF when absent
 };
 
 struct alignas(16) MaterialRecord {
@@ -77,7 +78,14 @@ struct alignas(16) MaterialRecord {
     float f0[3];
     float alpha;
     float eta;  // dielectric interior IOR
-    float pad[2];
+    int32_t tex;  // Lambertian albedo texture, -1: constant albedo
+    float pad;
+};
+
+// ImageTexture (src/texture.rs:65-151) texels [offset, offset + width * height)
+// of DevScene::texels, linear RGB, row-major from the top row.
+struct TextureRecord {
+    uint32_t offset, width, height, pad;
 };
 
 struct alignas(16) LightRecord {
@@ -104,6 +112,9 @@ struct DevScene {
     const LightRecord* lights;
     const float* light_cdf;
     const float* light_pmf;
+    const float* texcoords;
+    const float4* texels;
+    const TextureRecord* textures;
     uint32_t tlas_root;       // 0xFFFFFFFF: empty scene
     uint32_t num_lights;
     uint32_t light_dist;      // ar_light_distribution

@@ -52,9 +52,11 @@ struct BdParams {
     float4* va;  // p.xyz, pdf_fwd
     float4* vb;  // n.xyz, pdf_rev
     float4* vc;  // thr.xyz, info (type << 30 | delta << 29 | index)
-    float4* sva; // the three vertex arrays permuted into the (S, T)-sorted sample
+    float2* vuv; // tex_uv of surface vertices
+    float4* sva; // the vertex arrays permuted into the (S, T)-sorted sample
     float4* svb; // order, so the connection kernel's warps read them coalesced
     float4* svc;
+    float2* svuv;
     uint8_t* nv; // [sub * nsamples + si]
     float4* thr; // per subpath q = 2 si + sub: thr.xyz, previous directional pdf
     uint32_t* dim;
@@ -102,12 +104,23 @@ __device__ __forceinline__ Vtx load_vtx(const BdParams& P, uint32_t sub, uint32_
 }
 
 __device__ __forceinline__ void store_vtx(const BdParams& P, uint32_t sub, uint32_t k, uint32_t si, f3 p, f3 n, f3 thr,
-                                          float pdf_fwd, uint32_t type, bool delta, uint32_t index) {
+                                          float pdf_fwd, uint32_t type, bool delta, uint32_t index, float tu = 0.f,
+                                          float tv = 0.f) {
     const size_t i = vidx(P, sub, k, si);
     P.va[i] = make_float4(p.x, p.y, p.z, pdf_fwd);
     P.vb[i] = make_float4(n.x, n.y, n.z, 0.f);
     P.vc[i] = make_float4(thr.x, thr.y, thr.z,
                           __uint_as_float((type << 30) | (delta ? (1u << 29) : 0u) | (index & 0x1fffffffu)));
+    if (type == kTypeSurface) P.vuv[i] = make_float2(tu, tv);
+}
+
+// The material of surface vertex (sub, k) of sample si, with a textured
+// albedo sampled at the vertex's tex_uv (read only for textured materials).
+__device__ __forceinline__ MatView vtx_mat(const BdParams& P, const BdJob& J, const Vtx& v, uint32_t sub, uint32_t k,
+                                           uint32_t si) {
+    if (J.sc.materials[v.index].tex < 0) return load_mat(J.sc, v.index);
+    const float2 uv = P.vuv[vidx(P, sub, k, si)];
+    return load_mat_at(J.sc, v.index, uv.x, uv.y);
 }
 
 // pdf_solid_angle_to_area (:305-314) and geometry_term (:318-328)
@@ -397,7 +410,7 @@ __global__ void __launch_bounds__(256) k_bd_vertex(BdParams P, uint32_t depth) {
                 const float4 ro4 = P.ray_o[b][j], rd4 = P.ray_d[b][j];
                 const f3 ro = mk(ro4.x, ro4.y, ro4.z), rd = mk(rd4.x, rd4.y, rd4.z);
                 const Shade s = make_shade(J.sc, ro, rd, h.x, h.y, h.z, slot, P.hit_inst[j]);
-                const MatView m = load_mat(J.sc, s.mat);
+                const MatView m = load_mat_at(J.sc, s.mat, s.tu, s.tv);
                 const float4 t4 = P.thr[q];
                 f3 thr = mk(t4.x, t4.y, t4.z);
                 const uint32_t k = P.nv[sub * P.nsamples + si];  // index of the new vertex
@@ -405,7 +418,7 @@ __global__ void __launch_bounds__(256) k_bd_vertex(BdParams P, uint32_t depth) {
                 const float4 pa = P.va[pi], pb = P.vb[pi];
                 const f3 prev_p = mk(pa.x, pa.y, pa.z), prev_n = mk(pb.x, pb.y, pb.z);
                 const float pdf_fwd = pdf_sa_to_area(t4.w, prev_p, s.p, s.n);
-                store_vtx(P, sub, k, si, s.p, s.n, thr, pdf_fwd, kTypeSurface, false, s.mat);
+                store_vtx(P, sub, k, si, s.p, s.n, thr, pdf_fwd, kTypeSurface, false, s.mat, s.tu, s.tv);
                 P.nv[sub * P.nsamples + si] = uint8_t(k + 1);
                 const unsigned long long g = P.sindex[si];
                 const uint32_t npix = J.width * J.height;
@@ -468,7 +481,7 @@ __device__ __forceinline__ CamSide cam_side(const BdParams& P, const BdJob& J, u
     c.z = load_vtx(P, 0, s - 1, si);
     c.zp_p = load_vtx(P, 0, s - 2, si).p;
     c.oz = onb_from_normal(c.z.n);
-    c.mz = load_mat(J.sc, c.z.index);
+    c.mz = vtx_mat(P, J, c.z, 0, s - 1, si);
     c.wo_zl = to_local(c.oz, normalize(c.zp_p - c.z.p));
     return c;
 }
@@ -514,7 +527,7 @@ __device__ void connect_general(const BdParams& P, const BdJob& J, uint32_t job,
     f3 wo_yl = mk(0.f, 0.f, 0.f);
     if (t != 1) {
         oy = onb_from_normal(y.n);
-        my = load_mat(J.sc, y.index);
+        my = vtx_mat(P, J, y, 1, t - 1, si);
         const Vtx yp = load_vtx(P, 1, t - 2, si);
         wo_yl = to_local(oy, normalize(yp.p - y.p));
         f_y = bsdf_eval_ool(my, to_local(oy, wi_y), wo_yl);
@@ -577,7 +590,7 @@ __device__ void connect_s1(const BdParams& P, const BdJob& J, uint32_t job, uint
     const float c2 = ct * ct, c4 = c2 * c2;
     const float we = 1.0f / (J.cam.area * c4);
     const Onb oy = onb_from_normal(y.n);
-    const MatView my = load_mat(J.sc, y.index);
+    const MatView my = vtx_mat(P, J, y, 1, t - 1, si);
     const Vtx yp = load_vtx(P, 1, t - 2, si);
     const f3 wo_yl = to_local(oy, normalize(yp.p - y.p));
     const f3 f_y = bsdf_eval_ool(my, to_local(oy, wi), wo_yl);
@@ -656,6 +669,7 @@ __global__ void __launch_bounds__(256) k_bd_permute(BdParams P) {
                 P.sva[to] = P.va[from];
                 P.svb[to] = P.vb[from];
                 P.svc[to] = P.vc[from];
+                if (sub == 0 || k > 0) P.svuv[to] = P.vuv[from];  // surface vertices only
             }
         }
     }
@@ -747,7 +761,7 @@ struct BdptBatcher {
 
 size_t bdpt_batch_bytes(uint32_t max_depth, uint32_t batch) {
     const size_t maxv = max_depth + 1;
-    const size_t per_sample = 2 * 2 * maxv * 48 + 2 + 2 * (16 + 4) + 2 * 2 * (32 + 4) + 2 * 20 + 4 + 8 +
+    const size_t per_sample = 2 * 2 * maxv * 56 + 2 + 2 * (16 + 4) + 2 * 2 * (32 + 4) + 2 * 20 + 4 + 8 +
                               size_t(max_pairs_for(max_depth)) * 52 + 4;
     return per_sample * batch + 64 * 1024;
 }
@@ -773,9 +787,11 @@ BdptBatcher* bdpt_create(ar_context* ctx, uint32_t max_depth_cap, uint32_t batch
     P.va = carve<float4>(cur, nvtx);
     P.vb = carve<float4>(cur, nvtx);
     P.vc = carve<float4>(cur, nvtx);
+    P.vuv = carve<float2>(cur, nvtx);
     P.sva = carve<float4>(cur, nvtx);
     P.svb = carve<float4>(cur, nvtx);
     P.svc = carve<float4>(cur, nvtx);
+    P.svuv = carve<float2>(cur, nvtx);
     P.nv = carve<uint8_t>(cur, 2 * size_t(batch));
     P.thr = carve<float4>(cur, 2 * size_t(batch));
     P.dim = carve<uint32_t>(cur, 2 * size_t(batch));
@@ -868,6 +884,7 @@ void bdpt_run_batch(BdptBatcher* b, const std::vector<BdJob>& jobs, const std::v
         Pc.va = P.sva;
         Pc.vb = P.svb;
         Pc.vc = P.svc;
+        Pc.vuv = P.svuv;
         k_bd_connect<<<std::max(1, int(std::min<uint64_t>((nsamples + 127) / 128, ctx->num_sms * 16))), 128, 0,
                        ctx->stream>>>(Pc);
     }

@@ -216,7 +216,7 @@ __global__ void __launch_bounds__(256) k_shade(EngineDev E, int q) {
                 const float4 ro4 = B.ray_o[j], rd4 = B.ray_d[j];
                 const f3 ro = mk(ro4.x, ro4.y, ro4.z), rd = mk(rd4.x, rd4.y, rd4.z);
                 const Shade s = make_shade(sc, ro, rd, h.x, h.y, h.z, slot, E.hit_inst[j]);
-                const MatView m = load_mat(sc, s.mat);
+                const MatView m = load_mat_at(sc, s.mat, s.tu, s.tv);
                 const f3 wo = -rd;
                 const f3 wo_l = to_local(s.onb, wo);
                 const bool lights_on = light_enabled(sc);

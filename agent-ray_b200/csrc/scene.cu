@@ -223,7 +223,7 @@ void create_scene(ar_context* ctx, const ar_scene_desc* d, ar_scene** out) {
     AR_REQUIRE(d->light_distribution <= AR_LIGHT_DIST_POWER, AR_ERR_INVALID_ARGUMENT, "bad light distribution");
     // meshes
     std::vector<uint32_t> indices, slots;
-    std::vector<float> normals;
+    std::vector<float> normals, texcoords;
     std::vector<MeshRecord> mrec(d->num_meshes);
     uint64_t ntri_total = 0;
     s->meshes.resize(d->num_meshes);
@@ -247,6 +247,12 @@ void create_scene(ar_context* ctx, const ar_scene_desc* d, ar_scene** out) {
             normals.insert(normals.end(), md.normals, md.normals + 3 * size_t(md.num_vertices));
         } else {
             mrec[m].nrm_offset = kInvalid;
+        }
+        if (md.tex_coords) {
+            mrec[m].uv_offset = uint32_t(texcoords.size() / 2);
+            texcoords.insert(texcoords.end(), md.tex_coords, md.tex_coords + 2 * size_t(md.num_vertices));
+        } else {
+            mrec[m].uv_offset = kInvalid;
         }
         mrec[m].slot_offset = uint32_t(slots.size());
         if (md.num_material_slots == 0 || !md.material_slots) {
@@ -300,6 +306,9 @@ void create_scene(ar_context* ctx, const ar_scene_desc* d, ar_scene** out) {
         for (int k = 0; k < 3; ++k) { r.albedo[k] = m.albedo[k]; r.f0[k] = m.f0[k]; }
         r.alpha = std::min(1.0f, std::max(1e-3f, m.roughness));
         r.eta = m.eta;
+        AR_REQUIRE(m.albedo_texture < int32_t(d->num_textures), AR_ERR_INVALID_ARGUMENT,
+                   "albedo_texture out of range");
+        r.tex = m.kind == AR_MATERIAL_LAMBERTIAN ? std::max<int32_t>(m.albedo_texture, -1) : -1;
         s->materials_h[i] = r;
     }
     // lights + distribution (src/lights.rs:171-235)
@@ -347,6 +356,25 @@ void create_scene(ar_context* ctx, const ar_scene_desc* d, ar_scene** out) {
             s->cdf_h[n - 1] = 1.0f;
         }
     }
+    // ImageTexture::load (src/texture.rs:77-94): sRGB bytes -> linear f32
+    AR_REQUIRE(d->num_textures == 0 || d->textures, AR_ERR_INVALID_ARGUMENT, "textures is null");
+    std::vector<float4> texels;
+    std::vector<TextureRecord> trec(d->num_textures);
+    for (uint32_t t = 0; t < d->num_textures; ++t) {
+        const ar_texture_desc& td = d->textures[t];
+        AR_REQUIRE(td.rgb8 && td.width > 0 && td.height > 0, AR_ERR_INVALID_ARGUMENT, "empty texture");
+        AR_REQUIRE(uint64_t(td.width) * td.height < (1ull << 28), AR_ERR_INVALID_ARGUMENT, "texture too large");
+        trec[t] = TextureRecord{uint32_t(texels.size()), td.width, td.height, 0};
+        const auto lin = [](uint8_t b) {
+            const float x = float(b) / 255.0f;
+            return x <= 0.04045f ? x / 12.92f : std::pow((x + 0.055f) / 1.055f, 2.4f);
+        };
+        for (size_t i = 0; i < size_t(td.width) * td.height; ++i)
+            texels.push_back(make_float4(lin(td.rgb8[3 * i]), lin(td.rgb8[3 * i + 1]), lin(td.rgb8[3 * i + 2]), 0.f));
+    }
+    upload(s->texcoords, texcoords);
+    upload(s->texels, texels);
+    upload(s->textures, trec);
     upload(s->indices, indices);
     upload(s->normals, normals);
     upload(s->slots, slots);
@@ -361,6 +389,9 @@ void create_scene(ar_context* ctx, const ar_scene_desc* d, ar_scene** out) {
     s->view.meshes = s->meshes_d.as<MeshRecord>();
     s->view.indices = s->indices.as<uint32_t>();
     s->view.normals = s->normals.as<float>();
+    s->view.texcoords = s->texcoords.as<float>();
+    s->view.texels = s->texels.as<float4>();
+    s->view.textures = s->textures.as<TextureRecord>();
     s->view.material_slots = s->slots.as<uint32_t>();
     s->view.material_table = s->mat_table.as<uint32_t>();
     s->view.materials = s->materials.as<MaterialRecord>();
@@ -373,7 +404,8 @@ void create_scene(ar_context* ctx, const ar_scene_desc* d, ar_scene** out) {
     build_scene_accel(s.get(), nullptr);
     size_t bytes = 0;
     for (DevBuf* b : {&s->nodes, &s->tris, &s->instances, &s->objects_d, &s->meshes_d, &s->indices, &s->normals,
-                      &s->slots, &s->mat_table, &s->materials, &s->lights, &s->light_cdf, &s->light_pmf})
+                      &s->slots, &s->mat_table, &s->materials, &s->lights, &s->light_cdf, &s->light_pmf,
+                      &s->texcoords, &s->texels, &s->textures})
         bytes += b->bytes;
     s->stats.device_bytes = bytes;
     *out = s.release();

@@ -66,6 +66,8 @@ typedef struct ar_mesh_desc {
     const float* normals;            /* num_vertices * 3, or NULL (geometric normal is used) */
     const uint32_t* indices;         /* num_triangles * 3 */
     const uint32_t* material_slots;  /* 1 entry (shared slot) or num_triangles entries */
+    const float* tex_coords;         /* num_vertices * 2, or NULL: tex_uv is then the barycentric (u, v)
+                                        (SceneObject::tex_uv, src/scene.rs:54-66) */
     uint32_t num_vertices;
     uint32_t num_triangles;
     uint32_t num_material_slots;
@@ -98,7 +100,16 @@ typedef struct ar_material_desc {
     float f0[3];                     /* conductor reflectance at normal incidence */
     float roughness;                 /* conductor / dielectric GGX alpha, clamped to [1e-3, 1] */
     float eta;                       /* dielectric interior index of refraction (> 0) */
+    int32_t albedo_texture;          /* Lambertian: index into ar_scene_desc.textures (ImageTexture), or -1 */
+    uint32_t _pad;
 } ar_material_desc;
+
+/* ImageTexture (src/texture.rs:65-151): 8-bit sRGB texels, decoded to linear
+ * at scene creation, sampled bilinearly with repeat wrap. */
+typedef struct ar_texture_desc {
+    const uint8_t* rgb8;             /* width * height * 3 bytes, row-major from the top row */
+    uint32_t width, height;
+} ar_texture_desc;
 
 enum ar_light_kind {
     AR_LIGHT_POINT = 0,              /* src/lights/point.rs */
@@ -125,12 +136,13 @@ typedef struct ar_scene_desc {
     const ar_object_desc* objects;
     const ar_material_desc* materials;
     const ar_light_desc* lights;
+    const ar_texture_desc* textures;
     uint32_t num_meshes;
     uint32_t num_objects;
     uint32_t num_materials;
     uint32_t num_lights;
     uint32_t light_distribution;
-    uint32_t _pad;
+    uint32_t num_textures;
 } ar_scene_desc;
 
 /* PinholeCamera::from_lookat (src/cameras.rs:91-123). */

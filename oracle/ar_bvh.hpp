@@ -237,6 +237,7 @@ template <class T>
 struct MeshBlas {
     std::vector<V3<T>> pos;
     std::vector<V3<T>> nrm;  // empty if absent
+    std::vector<V2<T>> uv;   // tex_coords, empty if absent
     std::vector<uint32_t> idx;
     std::vector<uint32_t> slots;
     BuildResult bvh;

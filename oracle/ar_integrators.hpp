@@ -82,7 +82,7 @@ V3<T> pt_li(const Scene<T>& sc, Ray<T> ray, S& sampler, uint32_t max_depth, uint
                     V3<T> wi_l = hit.onb.to_local(ls.wi);
                     T cos_wi = std::fabs(wi_l.z);
                     if (cos_wi > T(0)) {
-                        V3<T> f = m.eval(wi_l, wo_l);
+                        V3<T> f = m.eval(wi_l, wo_l, hit.uv);
                         if (light.is_delta()) {
                             L += ((thr * f) * cos_wi) * ls.li / sel;
                         } else {
@@ -98,7 +98,7 @@ V3<T> pt_li(const Scene<T>& sc, Ray<T> ray, S& sampler, uint32_t max_depth, uint
         T u_sel = T(sampler.next_1d());
         V2<T> ud{T(sampler.next_1d()), T(0)};
         ud.y = T(sampler.next_1d());
-        BsdfSample<T> bs = m.sample(wo_l, u_sel, ud);
+        BsdfSample<T> bs = m.sample(wo_l, hit.uv, u_sel, ud);
         if (!bs.valid) break;
         if (bs.pdf == T(0) || bs.f == V3<T>(0, 0, 0)) break;
         T cos_wi = std::fabs(bs.wi.z);
@@ -162,6 +162,7 @@ struct PathVertex {
     T pdf_fwd, pdf_rev;
     bool is_delta;
     int32_t light;
+    V2<T> uv;  // tex_uv of surface vertices
     bool connectible() const { return type != V_SURFACE || !is_delta; }  // :281-292
 };
 
@@ -194,14 +195,14 @@ inline void bdpt_subpath_walk(const Scene<T>& sc, Ray<T> ray, V3<T> thr, T prev_
         ShadingPoint<T> hit;
         if (!sc.intersect(ray, hit)) break;
         T pdf_fwd = pdf_sa_to_area(prev_pdf_dir, vs.back().p, hit.p, hit.n);
-        PathVertex<T> v{V_SURFACE, hit.p, hit.n, hit.onb, hit.mat, thr, pdf_fwd, T(0), false, -1};
+        PathVertex<T> v{V_SURFACE, hit.p, hit.n, hit.onb, hit.mat, thr, pdf_fwd, T(0), false, -1, hit.uv};
         vs.push_back(v);
         V3<T> wo = -ray.d;
         V3<T> wo_l = hit.onb.to_local(wo);
         T u_sel = T(smp.next_1d());
         V2<T> ud{T(smp.next_1d()), T(0)};
         ud.y = T(smp.next_1d());
-        BsdfSample<T> bs = hit.mat->sample(wo_l, u_sel, ud);
+        BsdfSample<T> bs = hit.mat->sample(wo_l, hit.uv, u_sel, ud);
         if (!bs.valid) break;
         if (bs.pdf == T(0) || bs.f == V3<T>(0, 0, 0)) break;
         T cos_wi = std::fabs(bs.wi.z);
@@ -354,12 +355,12 @@ bool connect_bdpt(const Scene<T>& sc, const std::vector<PathVertex<T>>& cv, cons
     if (sc.occluded(sr)) return false;
     V3<T> wo_z = normalize(cv[s - 2].p - z.p);
     V3<T> wo_zl = z.onb.to_local(wo_z);
-    V3<T> f_z = z.mat ? z.mat->eval(z.onb.to_local(wi_z), wo_zl) : V3<T>(1, 1, 1);
+    V3<T> f_z = z.mat ? z.mat->eval(z.onb.to_local(wi_z), wo_zl, z.uv) : V3<T>(1, 1, 1);
     if (f_z == V3<T>(0, 0, 0)) return false;
     V3<T> f_y(1, 1, 1);
     if (t != 1 && y.mat) {
         V3<T> wo_y = normalize(lv[t - 2].p - y.p);
-        f_y = y.mat->eval(y.onb.to_local(wi_y), y.onb.to_local(wo_y));
+        f_y = y.mat->eval(y.onb.to_local(wi_y), y.onb.to_local(wo_y), y.uv);
     }
     if (f_y == V3<T>(0, 0, 0)) return false;
     T g = geometry_term(z.p, z.n, y.p, y.n);
@@ -370,7 +371,7 @@ bool connect_bdpt(const Scene<T>& sc, const std::vector<PathVertex<T>>& cv, cons
             // :951-967 — the reference re-samples the point light toward z.
             LightSample<T> ls = light.sample(z.p, V2<T>{T(0), T(0)});
             if (!ls.valid) return false;
-            V3<T> f_direct = z.mat ? z.mat->eval(z.onb.to_local(ls.wi), wo_zl) : V3<T>(1, 1, 1);
+            V3<T> f_direct = z.mat ? z.mat->eval(z.onb.to_local(ls.wi), wo_zl, z.uv) : V3<T>(1, 1, 1);
             T cos_z = std::fabs(dot(z.n, ls.wi));
             c = ((z.thr * f_direct) * cos_z) * ls.li;
         } else {
@@ -424,7 +425,7 @@ bool connect_s1(const Scene<T>& sc, const Camera<T>& cam, const std::vector<Path
     V3<T> f_y(1, 1, 1);
     V3<T> wo_y = normalize(lv[t - 2].p - y.p);
     V3<T> wo_yl = y.onb.to_local(wo_y);
-    if (y.mat) f_y = y.mat->eval(y.onb.to_local(to_cam), wo_yl);
+    if (y.mat) f_y = y.mat->eval(y.onb.to_local(to_cam), wo_yl, y.uv);
     if (f_y == V3<T>(0, 0, 0)) return false;
     T cos_y = std::fabs(dot(y.n, to_cam));
     T gf = cos_y / (dist * dist);

@@ -14,6 +14,8 @@
 
 namespace oracle {
 
+template <class T> struct V2 { T x, y; };
+
 template <class T>
 struct V3 {
     T x, y, z;

@@ -5,6 +5,8 @@
 //   Bsdf helpers                         src/surfaces.rs:36-83, :109-111
 //   Lambertian                           src/surfaces/lambertian.rs:35-64
 //   ConductorBsdf + GGX                  src/surfaces/microfacet.rs:14-152
+//   DielectricBsdf                       src/surfaces/microfacet.rs:155-307, src/surfaces.rs:86-123
+//   ImageTexture                         src/texture.rs:65-151
 //   Light / PointLight                   src/lights.rs:14-103, src/lights/point.rs:48-100
 //   Uniform/PowerLightDistribution       src/lights.rs:136-235
 //   PinholeCamera                        src/cameras.rs:91-248
@@ -19,7 +21,6 @@
 
 namespace oracle {
 
-template <class T> struct V2 { T x, y; };
 
 // Onb::from_normal (src/geometry.rs:218-232)
 template <class T>
@@ -124,6 +125,48 @@ inline bool refract(V3<T> v, V3<T> n, T eta, V3<T>& out) {
     return true;
 }
 
+// src/texture.rs:139-150 (IEC 61966-2-1), in f32 as the reference decodes
+inline float srgb_to_linear(float x) { return x <= 0.04045f ? x / 12.92f : std::pow((x + 0.055f) / 1.055f, 2.4f); }
+
+// ImageTexture (src/texture.rs:65-136): linear texels, bilinear, repeat wrap.
+template <class T>
+struct Texture {
+    std::vector<V3<T>> data;  // row-major, top row first
+    uint32_t width = 0, height = 0;
+
+    void load(const ar_texture_desc& d) {
+        width = d.width;
+        height = d.height;
+        data.resize(size_t(width) * height);
+        for (size_t i = 0; i < data.size(); ++i)
+            data[i] = V3<T>(T(srgb_to_linear(float(d.rgb8[3 * i]) / 255.0f)),
+                            T(srgb_to_linear(float(d.rgb8[3 * i + 1]) / 255.0f)),
+                            T(srgb_to_linear(float(d.rgb8[3 * i + 2]) / 255.0f)));
+    }
+    static T wrap01(T x) {  // x.fract().rem_euclid(1.0)
+        T f = x - std::trunc(x);
+        T r = std::fmod(f, T(1));
+        return r < T(0) ? r + T(1) : r;
+    }
+    V3<T> fetch(int32_t x, int32_t y) const {
+        const int32_t w = int32_t(width), h = int32_t(height);
+        int32_t xm = x % w, ym = y % h;
+        if (xm < 0) xm += w;
+        if (ym < 0) ym += h;
+        return data[size_t(uint32_t(ym) * width + uint32_t(xm))];
+    }
+    V3<T> sample(V2<T> uv) const {
+        T u = wrap01(uv.x) * T(float(width)) - T(0.5f);
+        T v = wrap01(uv.y) * T(float(height)) - T(0.5f);
+        T fu = std::floor(u), fv = std::floor(v);
+        int32_t x0 = int32_t(fu), y0 = int32_t(fv);
+        T tx = u - fu, ty = v - fv;
+        V3<T> c00 = fetch(x0, y0), c10 = fetch(x0 + 1, y0), c01 = fetch(x0, y0 + 1), c11 = fetch(x0 + 1, y0 + 1);
+        return ((c00 * ((T(1) - tx) * (T(1) - ty)) + c10 * (tx * (T(1) - ty))) + c01 * ((T(1) - tx) * ty)) +
+               c11 * (tx * ty);
+    }
+};
+
 template <class T>
 struct BsdfSample {
     V3<T> wi;
@@ -139,6 +182,9 @@ struct Material {
     V3<T> albedo, f0;
     T alpha;
     T eta;                // DielectricBsdf interior IOR
+    const Texture<T>* tex = nullptr;  // Lambertian ImageTexture albedo, or constant `albedo`
+
+    V3<T> albedo_at(V2<T> uv) const { return tex ? tex->sample(uv) : albedo; }
 
     // DielectricBsdf (src/surfaces/microfacet.rs:155-307)
     V3<T> refraction_half(V3<T> wi, V3<T> wo, T e) const {
@@ -189,11 +235,11 @@ struct Material {
         return (((((f * ggx_d(alpha, h)) * abs_cos_theta(h)) * e) * e) * std::fabs(wih)) / denom;
     }
 
-    V3<T> eval(V3<T> wi, V3<T> wo) const {
+    V3<T> eval(V3<T> wi, V3<T> wo, V2<T> uv) const {
         if (kind == AR_MATERIAL_DIELECTRIC) return dielectric_eval(wi, wo);
         if (kind == AR_MATERIAL_LAMBERTIAN) {
             if (!same_hemisphere(wi, wo)) return {};
-            return albedo * frac_1_pi<T>();
+            return albedo_at(uv) * frac_1_pi<T>();
         }
         if (!same_hemisphere(wi, wo)) return {};
         T ci = abs_cos_theta(wi), co = abs_cos_theta(wo);
@@ -216,7 +262,7 @@ struct Material {
         if (whwi == T(0)) return T(0);
         return ggx_d(alpha, h) * abs_cos_theta(h) / (T(4) * whwi);
     }
-    BsdfSample<T> sample(V3<T> wo, T u_sel, V2<T> u) const {
+    BsdfSample<T> sample(V3<T> wo, V2<T> uv, T u_sel, V2<T> u) const {
         BsdfSample<T> s{};
         s.valid = false;
         if (kind == AR_MATERIAL_LAMBERTIAN) {
@@ -224,7 +270,7 @@ struct Material {
             if (wo.z < T(0)) wi.z = -wi.z;
             T pdf = abs_cos_theta(wi) * frac_1_pi<T>();
             if (pdf == T(0)) return s;
-            s = {wi, pdf, albedo * frac_1_pi<T>(), true};
+            s = {wi, pdf, albedo_at(uv) * frac_1_pi<T>(), true};
             return s;
         }
         if (wo.z == T(0)) return s;
@@ -237,14 +283,14 @@ struct Material {
             if (same_hemisphere(wi, wo)) return s;
             T p = pdf(wi, wo);
             if (p == T(0)) return s;
-            s = {wi, p, eval(wi, wo), true};
+            s = {wi, p, eval(wi, wo, uv), true};
             return s;
         }
         V3<T> wi = reflect(wo, h);
         if (!same_hemisphere(wi, wo)) return s;
         T p = pdf(wi, wo);
         if (p == T(0)) return s;
-        s = {wi, p, eval(wi, wo), true};
+        s = {wi, p, eval(wi, wo, uv), true};
         return s;
     }
 };
@@ -559,6 +605,7 @@ struct Object {
 template <class T>
 struct ShadingPoint {
     V3<T> p, n;
+    V2<T> uv;  // tex_uv (src/scene.rs:54-66)
     Onb<T> onb;
     const Material<T>* mat;
     uint32_t inst, prim;
@@ -571,6 +618,7 @@ struct Scene {
     std::vector<Object<T>> objects;
     std::vector<Material<T>> materials;
     std::vector<Light<T>> lights;
+    std::vector<Texture<T>> textures;
     LightDist<T> ldist;
     BuildResult tlas;
 
@@ -586,6 +634,11 @@ struct Scene {
                 mb.nrm.resize(md.num_vertices);
                 for (uint32_t i = 0; i < md.num_vertices; ++i)
                     mb.nrm[i] = V3<T>(T(md.normals[3 * i]), T(md.normals[3 * i + 1]), T(md.normals[3 * i + 2]));
+            }
+            if (md.tex_coords) {
+                mb.uv.resize(md.num_vertices);
+                for (uint32_t i = 0; i < md.num_vertices; ++i)
+                    mb.uv[i] = V2<T>{T(md.tex_coords[2 * i]), T(md.tex_coords[2 * i + 1])};
             }
             mb.idx.assign(md.indices, md.indices + 3 * size_t(md.num_triangles));
             if (md.num_material_slots == 0 || !md.material_slots) mb.slots = {0u};
@@ -611,6 +664,8 @@ struct Scene {
             ob.mats.assign(od.materials, od.materials + od.num_materials);
             ob.world = transform_aabb(meshes[ob.mesh].overall, ob.xf);
         }
+        textures.resize(d.num_textures);
+        for (uint32_t i = 0; i < d.num_textures; ++i) textures[i].load(d.textures[i]);
         materials.resize(d.num_materials);
         for (uint32_t i = 0; i < d.num_materials; ++i) {
             const auto& m = d.materials[i];
@@ -622,6 +677,8 @@ struct Scene {
             float a = m.roughness < 1e-3f ? 1e-3f : (m.roughness > 1.0f ? 1.0f : m.roughness);
             mm.alpha = T(a);
             mm.eta = T(m.eta);
+            mm.tex = m.albedo_texture >= 0 && uint32_t(m.albedo_texture) < textures.size()
+                         ? &textures[m.albedo_texture] : nullptr;
         }
         lights.resize(d.num_lights);
         for (uint32_t i = 0; i < d.num_lights; ++i) {
@@ -681,6 +738,14 @@ struct Scene {
         if (dot(n, wo) < T(0)) n = -n;
         sp.n = n;
         sp.onb = Onb<T>::from_normal(n);
+        if (!m.uv.empty()) {  // tex_coords[i0] * w + tex_coords[i1] * u + tex_coords[i2] * v
+            uint32_t i0 = m.idx[3 * h.prim], i1 = m.idx[3 * h.prim + 1], i2 = m.idx[3 * h.prim + 2];
+            T w = (T(1) - h.u) - h.v;
+            sp.uv = V2<T>{(m.uv[i0].x * w + m.uv[i1].x * h.u) + m.uv[i2].x * h.v,
+                          (m.uv[i0].y * w + m.uv[i1].y * h.u) + m.uv[i2].y * h.v};
+        } else {
+            sp.uv = V2<T>{h.u, h.v};
+        }
         uint32_t slot = m.slots.size() == 1 ? m.slots[0] : m.slots[h.prim];
         size_t k = std::min<size_t>(slot, ob.mats.size() - 1);
         sp.mat = &materials[ob.mats[k]];

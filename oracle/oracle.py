@@ -43,6 +43,7 @@ def lib():
         lb.oracle_xoshiro_f32.argtypes = [u32, u32, u32, vp]
         lb.oracle_blas_stats.argtypes = [vp, u32, vp]
         lb.oracle_film_to_rgb8.argtypes = [vp, u32, u32, u32, C.c_float, C.c_float, C.c_float, vp]
+        lb.oracle_texture_sample.argtypes = [vp, u32, u32, vp, u32, vp]
         _lib = lb
     return _lib
 
@@ -163,3 +164,13 @@ def film_to_rgb8(hdr, tone_mapper=0, white_point=1.0, gamma=2.2, scale=1.0):
     lib().oracle_film_to_rgb8(_p(x), w, h, tone_mapper, white_point, gamma, scale, _p(out))
     return out
 
+
+
+def texture_sample(rgb8, uv):
+    """ImageTexture::sample of an (H, W, 3) uint8 sRGB image at (N, 2) uv -> (N, 3) float32."""
+    img = np.ascontiguousarray(rgb8, np.uint8)
+    q = np.ascontiguousarray(uv, np.float32).reshape(-1, 2)
+    out = np.empty((q.shape[0], 3), np.float32)
+    rc = lib().oracle_texture_sample(_p(img), img.shape[1], img.shape[0], _p(q), q.shape[0], _p(out))
+    assert rc == 0
+    return out

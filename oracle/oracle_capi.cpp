@@ -190,6 +190,20 @@ int oracle_film_to_rgb8(const float* hdr, uint32_t w, uint32_t h, uint32_t tm, f
     return 0;
 }
 
+// ImageTexture::load + sample (src/texture.rs:77-136) at n uv pairs, in f32.
+int oracle_texture_sample(const uint8_t* rgb8, uint32_t w, uint32_t h, const float* uv, uint32_t n, float* out) {
+    if (!rgb8 || w == 0 || h == 0) return 1;
+    Texture<float> t;
+    t.load(ar_texture_desc{rgb8, w, h});
+    for (uint32_t i = 0; i < n; ++i) {
+        const V3<float> c = t.sample(V2<float>{uv[2 * i], uv[2 * i + 1]});
+        out[3 * i] = c.x;
+        out[3 * i + 1] = c.y;
+        out[3 * i + 2] = c.z;
+    }
+    return 0;
+}
+
 // First n f32 draws of the pixel-seeded independent sampler (xoshiro256++).
 int oracle_xoshiro_f32(uint32_t px, uint32_t py, uint32_t n, float* out) {
     Sampler s(SAMPLER_XOSHIRO, px, py, 1, 0);

@@ -15,6 +15,7 @@ src/cameras.rs, src/film.rs) maps as follows:
 All work runs in the CUDA library; nothing here computes on the CPU.
 """
 import ctypes as C
+import os
 from dataclasses import dataclass
 
 import numpy as np
@@ -188,6 +189,10 @@ class Film:
     def save_png(self, path, tone_mapper=A.TONEMAP_CLAMP, gamma=2.2, scale=1.0, white_point=1.0):
         write_png(path, self.to_rgb_image(tone_mapper, gamma, scale, white_point))
 
+    def save_exr(self, path, scale=1.0):
+        """Film::save_exr (src/film.rs:304-346): linear HALF RGB, ZIP-compressed OpenEXR."""
+        film_save_exr(self.ctx, self.rgb, path, scale)
+
 
 def film_to_rgb8(ctx, hdr, tone_mapper=A.TONEMAP_CLAMP, gamma=2.2, scale=1.0, white_point=1.0):
     """Tone-maps an (H, W, 3) float32 image (host array or CUDA tensor) to
@@ -197,6 +202,7 @@ def film_to_rgb8(ctx, hdr, tone_mapper=A.TONEMAP_CLAMP, gamma=2.2, scale=1.0, wh
         raise ValueError("a Context is needed to tone-map on the GPU")
     if not isinstance(hdr, np.ndarray):
         import torch
+        hdr = hdr.to(torch.float32).contiguous()
         h, w = hdr.shape[0], hdr.shape[1]
         out = torch.empty((h, w, 3), dtype=torch.uint8, device=hdr.device)
         check(lib().ar_film_to_rgb8(ctx.handle, hdr.data_ptr(), w, h, tone_mapper, white_point, gamma, scale,
@@ -208,6 +214,21 @@ def film_to_rgb8(ctx, hdr, tone_mapper=A.TONEMAP_CLAMP, gamma=2.2, scale=1.0, wh
     check(lib().ar_film_to_rgb8(ctx.handle, x.ctypes.data, w, h, tone_mapper, white_point, gamma, scale,
                                 out.ctypes.data, 0))
     return out
+
+
+def film_save_exr(ctx, hdr, path, scale=1.0):
+    """Writes an (H, W, 3) float32 image (host array or CUDA tensor) * scale as
+    a ZIP-compressed HALF OpenEXR file with ar_film_save_exr."""
+    if ctx is None:
+        raise ValueError("a Context is needed to pack the EXR on the GPU")
+    p = os.fsencode(path)
+    if not isinstance(hdr, np.ndarray):
+        import torch
+        x = hdr.to(torch.float32).contiguous()
+        check(lib().ar_film_save_exr(ctx.handle, x.data_ptr(), x.shape[1], x.shape[0], scale, 1, p))
+        return
+    x = np.ascontiguousarray(hdr, np.float32)
+    check(lib().ar_film_save_exr(ctx.handle, x.ctypes.data, x.shape[1], x.shape[0], scale, 0, p))
 
 
 def write_png(path, rgb8):

@@ -25,6 +25,8 @@ SIGNATURES = {
     "ar_context_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(A.Tuning)]),
     "ar_film_to_rgb8": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.c_float,
                                   C.c_float, C.c_void_p, C.c_uint32]),
+    "ar_film_save_exr": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_float, C.c_uint32,
+                                   C.c_char_p]),
     "ar_context_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(A.Tuning)]),
     "ar_autotune": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(A.CameraDesc), C.POINTER(A.TuneOpts),
                               C.POINTER(A.TuneResult)]),

@@ -85,6 +85,7 @@ struct Vtx {
     float pdf_fwd, pdf_rev;
     uint32_t type, index;
     bool delta;
+    bool uv;  // a textured surface vertex: its tex_uv is stored in vuv
 };
 
 __device__ __forceinline__ Vtx load_vtx(const BdParams& P, uint32_t sub, uint32_t k, uint32_t si) {
@@ -99,26 +100,28 @@ __device__ __forceinline__ Vtx load_vtx(const BdParams& P, uint32_t sub, uint32_
     const uint32_t info = __float_as_uint(c.w);
     v.type = info >> 30;
     v.delta = (info >> 29) & 1u;
-    v.index = info & 0x1fffffffu;
+    v.uv = (info >> 28) & 1u;
+    v.index = info & 0x0fffffffu;
     return v;
 }
 
 __device__ __forceinline__ void store_vtx(const BdParams& P, uint32_t sub, uint32_t k, uint32_t si, f3 p, f3 n, f3 thr,
-                                          float pdf_fwd, uint32_t type, bool delta, uint32_t index, float tu = 0.f,
-                                          float tv = 0.f) {
+                                          float pdf_fwd, uint32_t type, bool delta, uint32_t index, bool uv = false,
+                                          float tu = 0.f, float tv = 0.f) {
     const size_t i = vidx(P, sub, k, si);
     P.va[i] = make_float4(p.x, p.y, p.z, pdf_fwd);
     P.vb[i] = make_float4(n.x, n.y, n.z, 0.f);
     P.vc[i] = make_float4(thr.x, thr.y, thr.z,
-                          __uint_as_float((type << 30) | (delta ? (1u << 29) : 0u) | (index & 0x1fffffffu)));
-    if (type == kTypeSurface) P.vuv[i] = make_float2(tu, tv);
+                          __uint_as_float((type << 30) | (delta ? (1u << 29) : 0u) | (uv ? (1u << 28) : 0u) |
+                                          (index & 0x0fffffffu)));
+    if (uv) P.vuv[i] = make_float2(tu, tv);
 }
 
 // The material of surface vertex (sub, k) of sample si, with a textured
 // albedo sampled at the vertex's tex_uv (read only for textured materials).
 __device__ __forceinline__ MatView vtx_mat(const BdParams& P, const BdJob& J, const Vtx& v, uint32_t sub, uint32_t k,
                                            uint32_t si) {
-    if (J.sc.materials[v.index].tex < 0) return load_mat(J.sc, v.index);
+    if (!v.uv) return load_mat(J.sc, v.index);
     const float2 uv = P.vuv[vidx(P, sub, k, si)];
     return load_mat_at(J.sc, v.index, uv.x, uv.y);
 }
@@ -418,7 +421,8 @@ __global__ void __launch_bounds__(256) k_bd_vertex(BdParams P, uint32_t depth) {
                 const float4 pa = P.va[pi], pb = P.vb[pi];
                 const f3 prev_p = mk(pa.x, pa.y, pa.z), prev_n = mk(pb.x, pb.y, pb.z);
                 const float pdf_fwd = pdf_sa_to_area(t4.w, prev_p, s.p, s.n);
-                store_vtx(P, sub, k, si, s.p, s.n, thr, pdf_fwd, kTypeSurface, false, s.mat, s.tu, s.tv);
+                store_vtx(P, sub, k, si, s.p, s.n, thr, pdf_fwd, kTypeSurface, false, s.mat,
+                          J.sc.materials[s.mat].tex >= 0, s.tu, s.tv);
                 P.nv[sub * P.nsamples + si] = uint8_t(k + 1);
                 const unsigned long long g = P.sindex[si];
                 const uint32_t npix = J.width * J.height;
@@ -668,8 +672,9 @@ __global__ void __launch_bounds__(256) k_bd_permute(BdParams P) {
                 const size_t from = vidx(P, sub, k, si), to = vidx(P, sub, k, oi);
                 P.sva[to] = P.va[from];
                 P.svb[to] = P.vb[from];
-                P.svc[to] = P.vc[from];
-                if (sub == 0 || k > 0) P.svuv[to] = P.vuv[from];  // surface vertices only
+                const float4 c = P.vc[from];
+                P.svc[to] = c;
+                if ((__float_as_uint(c.w) >> 28) & 1u) P.svuv[to] = P.vuv[from];  // textured vertices only
             }
         }
     }

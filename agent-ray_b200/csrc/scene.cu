@@ -220,6 +220,8 @@ void create_scene(ar_context* ctx, const ar_scene_desc* d, ar_scene** out) {
     AR_REQUIRE(d->num_objects == 0 || d->objects, AR_ERR_INVALID_ARGUMENT, "objects is null");
     AR_REQUIRE(d->num_materials > 0 && d->materials, AR_ERR_INVALID_ARGUMENT, "scene needs at least one material");
     AR_REQUIRE(d->num_lights == 0 || d->lights, AR_ERR_INVALID_ARGUMENT, "lights is null");
+    AR_REQUIRE(d->num_materials < (1u << 28) && d->num_lights < (1u << 28), AR_ERR_INVALID_ARGUMENT,
+               "at most 2^28 - 1 materials and lights (BDPT vertices pack the index in 28 bits)");
     AR_REQUIRE(d->light_distribution <= AR_LIGHT_DIST_POWER, AR_ERR_INVALID_ARGUMENT, "bad light distribution");
     // meshes
     std::vector<uint32_t> indices, slots;

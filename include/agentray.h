@@ -330,6 +330,15 @@ enum ar_tone_mapper {
 int ar_film_to_rgb8(ar_context* ctx, const float* hdr_rgb, uint32_t width, uint32_t height, uint32_t tone_mapper,
                     float white_point, float gamma, float scale, uint8_t* out_rgb8, uint32_t on_device);
 
+/* Film::save_exr (src/film.rs:304-346): writes linear RGB * scale, without
+ * tone mapping, to `path` as an OpenEXR scanline file with HALF channels
+ * B, G, R (f16 round-to-nearest-even) and ZIP compression (16 scanlines per
+ * chunk).  The f16 conversion, channel split and ZIP byte reorder + predictor
+ * run on the device; deflate runs on host threads.  `hdr_rgb` is a host
+ * pointer, or a device pointer with on_device = 1. */
+int ar_film_save_exr(ar_context* ctx, const float* hdr_rgb, uint32_t width, uint32_t height, float scale,
+                     uint32_t on_device, const char* path);
+
 /* screened_poisson_reconstruct (src/integrators/gradient_domain_pt.rs:449-630):
  * reconstructs an image from interleaved-RGB primal and forward-difference
  * gradient films (W*H*3 f32 each) with cfg->alpha and cfg->poisson_solver

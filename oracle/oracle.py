@@ -174,3 +174,57 @@ def texture_sample(rgb8, uv):
     rc = lib().oracle_texture_sample(_p(img), img.shape[1], img.shape[0], _p(q), q.shape[0], _p(out))
     assert rc == 0
     return out
+
+
+def f32_to_f16_bits(x):
+    """half::f16::from_f32 on float32 values -> uint16 bits: IEEE round to
+    nearest even; a NaN keeps its sign and top 10 mantissa bits with the quiet bit set."""
+    x = np.asarray(x, np.float32)
+    with np.errstate(over="ignore", invalid="ignore"):
+        bits = x.astype(np.float16).view(np.uint16).copy()
+    nan = np.isnan(x)
+    if nan.any():
+        b = x.view(np.uint32)[nan]
+        bits[nan] = (((b >> 16) & 0x8000) | 0x7E00 | ((b & 0x7FFFFF) >> 13)).astype(np.uint16)
+    return bits
+
+
+def film_save_exr(hdr, path, scale=1.0):
+    """Film::save_exr (src/film.rs:304-346) restated: (H, W, 3) float32 * scale
+    as HALF B/G/R channels of a single-part scanline OpenEXR file, ZIP
+    compression (16 scanlines per chunk; byte reorder, +128 delta predictor,
+    zlib at the default level; a chunk deflate does not shrink is stored raw),
+    attributes in name order, the layer named "beauty"."""
+    import struct
+    import zlib
+    h, w, _ = hdr.shape
+    with np.errstate(invalid="ignore"):
+        v = f32_to_f16_bits(np.asarray(hdr, np.float32) * np.float32(scale))  # (H, W, 3)
+    planar = np.ascontiguousarray(v[:, :, ::-1].transpose(0, 2, 1))  # (H, [B, G, R], W)
+
+    def attr(name, typ, data):
+        return name.encode() + b"\0" + typ.encode() + b"\0" + struct.pack("<i", len(data)) + data
+    ch = b"".join(c + b"\0" + struct.pack("<iIii", 1, 0, 1, 1) for c in (b"B", b"G", b"R")) + b"\0"
+    box = struct.pack("<4i", 0, 0, w - 1, h - 1)
+    head = (struct.pack("<II", 20000630, 2) + attr("channels", "chlist", ch) +
+            attr("compression", "compression", b"\x03") + attr("dataWindow", "box2i", box) +
+            attr("displayWindow", "box2i", box) + attr("lineOrder", "lineOrder", b"\x00") +
+            attr("name", "string", b"beauty") + attr("pixelAspectRatio", "float", struct.pack("<f", 1.0)) +
+            attr("screenWindowCenter", "v2f", struct.pack("<2f", 0.0, 0.0)) +
+            attr("screenWindowWidth", "float", struct.pack("<f", 1.0)) + b"\0")
+    chunks = []
+    for y0 in range(0, h, 16):
+        raw = planar[y0:y0 + 16].astype("<u2").tobytes()
+        r = np.frombuffer(raw, np.uint8)
+        t = np.concatenate([r[0::2], r[1::2]]).astype(np.int32)
+        t[1:] = (t[1:] - t[:-1] + 384) & 0xFF
+        z = zlib.compress(t.astype(np.uint8).tobytes(), 6)
+        chunks.append((y0, z if len(z) < len(raw) else raw))
+    offs, at = [], len(head) + 8 * len(chunks)
+    for y0, d in chunks:
+        offs.append(at)
+        at += 8 + len(d)
+    out = head + struct.pack("<%dQ" % len(offs), *offs) + b"".join(
+        struct.pack("<ii", y0, len(d)) + d for y0, d in chunks)
+    with open(path, "wb") as f:
+        f.write(out)

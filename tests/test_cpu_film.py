@@ -1,9 +1,13 @@
-"""Film output (Film::to_rgb_image, src/film.rs:136-302): the oracle's
-restatement against an independent numpy restatement, and the PNG writer."""
+"""Film output (Film::to_rgb_image, src/film.rs:136-302; Film::save_exr,
+:304-346): the oracle's tone-mapping restatement against an independent numpy
+restatement, the PNG writer, and the oracle's EXR writer read back by
+OpenCV's OpenEXR reader."""
+import os
 import struct
 import zlib
 
 import numpy as np
+import pytest
 
 import agentray
 import oracle as O
@@ -58,3 +62,53 @@ def test_png_round_trip(tmp_path):
     rows = [raw[r * 22 + 1:(r + 1) * 22] for r in range(6)]
     assert all(raw[r * 22] == 0 for r in range(6))
     np.testing.assert_array_equal(np.frombuffer(b"".join(rows), np.uint8).reshape(6, 7, 3), img)
+
+
+def _cv2_read_exr(path):
+    os.environ.setdefault("OPENCV_IO_ENABLE_OPENEXR", "1")
+    cv2 = pytest.importorskip("cv2")
+    img = cv2.imread(str(path), cv2.IMREAD_UNCHANGED)
+    assert img is not None, "OpenCV could not read the EXR file"
+    return img[:, :, ::-1]  # BGR -> RGB
+
+
+def _exr_attrs(data):
+    pos, attrs = 8, {}
+    while data[pos] != 0:
+        e = data.index(b"\0", pos)
+        name = data[pos:e].decode()
+        e2 = data.index(b"\0", e + 1)
+        typ = data[e + 1:e2].decode()
+        n = struct.unpack("<i", data[e2 + 1:e2 + 5])[0]
+        attrs[name] = (typ, data[e2 + 5:e2 + 5 + n])
+        pos = e2 + 5 + n
+    return attrs, pos + 1
+
+
+@pytest.mark.parametrize("h,w", [(37, 29), (16, 5), (1, 1), (33, 64)])
+def test_oracle_exr_read_back_by_opencv(tmp_path, h, w):
+    # Film::save_exr restated: OpenCV's OpenEXR reader (an independent
+    # implementation) gets back exactly the f16-rounded values.
+    rng = np.random.default_rng(h * 100 + w)
+    hdr = rng.lognormal(-1.0, 2.0, (h, w, 3)).astype(np.float32)
+    hdr.reshape(-1)[:3] = [0.0, 7e4, 3e-6]  # zero, f16 overflow (inf), an f16 subnormal
+    p = tmp_path / "o.exr"
+    O.film_save_exr(hdr, str(p), scale=0.5)
+    want = (hdr * np.float32(0.5)).astype(np.float16).astype(np.float32)
+    got = _cv2_read_exr(p)
+    np.testing.assert_array_equal(got, want)
+    data = p.read_bytes()
+    assert struct.unpack("<II", data[:8]) == (20000630, 2)
+    attrs, end = _exr_attrs(data)
+    assert attrs["compression"] == ("compression", b"\x03")
+    assert attrs["name"] == ("string", b"beauty")
+    assert struct.unpack("<4i", attrs["dataWindow"][1]) == (0, 0, w - 1, h - 1)
+    assert len(data) > end + 8 * ((h + 15) // 16)
+
+
+def test_f16_nan_rule():
+    x = np.array([np.nan, -np.nan, 1.0, 65520.0, 65519.0, 5.96e-8, -0.0], np.float32)
+    x[1] = np.frombuffer(np.uint32(0xFFC12345).tobytes(), np.float32)[0]
+    b = O.f32_to_f16_bits(x)
+    assert b[0] == 0x7E00 and b[1] == (0x8000 | 0x7E00 | (0x412345 >> 13))
+    assert b[2] == 0x3C00 and b[3] == 0x7C00 and b[4] == 0x7BFF and b[5] == 0x0001 and b[6] == 0x8000

@@ -62,25 +62,22 @@ def read_png(path):
             out[y] = cur
             prev = cur
             continue
-        cur = np.zeros(stride, np.int32)
+        # average / Paeth depend on the reconstructed left neighbour: a scalar
+        # loop over Python ints (several times faster than numpy scalars)
+        ln, up, cur = line.tolist(), prev.tolist(), [0] * stride
         for x in range(stride):
             a = cur[x - channels] if x >= channels else 0
-            b = prev[x]
-            c = prev[x - channels] if x >= channels else 0
-            if f == 0:
-                p = 0
-            elif f == 1:
-                p = a
-            elif f == 2:
-                p = b
-            elif f == 3:
-                p = (a + b) // 2
+            b = up[x]
+            if f == 3:
+                p = (a + b) >> 1
             elif f == 4:
+                c = up[x - channels] if x >= channels else 0
                 pa, pb, pc = abs(b - c), abs(a - c), abs(a + b - 2 * c)
                 p = a if pa <= pb and pa <= pc else (b if pb <= pc else c)
             else:
                 raise ValueError(f"bad PNG filter {f}")
-            cur[x] = (line[x] + p) & 0xFF
+            cur[x] = (ln[x] + p) & 0xFF
+        cur = np.array(cur, np.int32)
         out[y] = cur
         prev = cur
     px = out.reshape(h, w, channels)
@@ -103,6 +100,9 @@ def _luminance(c):
 
 
 def parse_mtl(path):
+    """The MTL statements the reference's conversion reads, as tobj parses them
+    (Kd, Ks, Ns, Ni, d, map_Kd; `Tr` is not read, so only `d` makes a
+    material transparent)."""
     mats, cur = {}, None
     for raw in open(path, encoding="utf-8", errors="replace"):
         t = raw.strip().split()
@@ -118,10 +118,8 @@ def parse_mtl(path):
             cur[key] = [float(x) for x in args[:3]]
         elif key in ("Ns", "Ni", "d"):
             cur[key] = float(args[0])
-        elif key == "Tr":
-            cur["d"] = 1.0 - float(args[0])
-        elif key == "map_Kd":
-            cur["map_Kd"] = args[-1]
+        elif key == "map_Kd":  # the rest of the line, as tobj reads it
+            cur["map_Kd"] = raw.strip()[len("map_Kd"):].strip()
     return mats
 
 

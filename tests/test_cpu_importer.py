@@ -2,6 +2,7 @@
 (src/importer.rs:75-241): the oracle's texture sampling against a numpy
 restatement, the PNG decoder against every filter type, and the importer's
 triangulation, single-index remap, model split and material rules."""
+import os
 import struct
 import zlib
 
@@ -137,8 +138,11 @@ newmtl plain
 Kd 0.25 0.5 0.75
 Ks 0.01 0.01 0.01
 newmtl lowni
-Tr 0.9
+d 0.1
 Ni 0.5
+newmtl tr_only
+Tr 0.9
+Kd 0.2 0.2 0.2
 """
 
 OBJ = """mtllib scene.mtl
@@ -183,6 +187,7 @@ def test_material_rules(tmp_path):
     assert mats["broken"].albedo_texture == -1 and mats["broken"].albedo == pytest.approx((0.3, 0.4, 0.5))
     assert mats["plain"].kind == A.MATERIAL_LAMBERTIAN and mats["plain"].albedo == pytest.approx((0.25, 0.5, 0.75))
     assert mats["lowni"].kind == A.MATERIAL_DIELECTRIC and mats["lowni"].eta == 1.0  # Ni clamped to >= 1
+    assert mats["tr_only"].kind == A.MATERIAL_LAMBERTIAN  # tobj does not read Tr
 
 
 def test_load_obj_scene_structure(tmp_path):
@@ -195,7 +200,7 @@ def test_load_obj_scene_structure(tmp_path):
     xf = np.eye(4, dtype=np.float32)
     xf[:3, 3] = [1.0, 2.0, 3.0]
     objs = I.load_obj_scene(sc, str(tmp_path / "scene.obj"), xf)
-    assert len(objs) == 4 and len(sc.materials) == 6 and len(sc.textures) == 1
+    assert len(objs) == 4 and len(sc.materials) == 7 and len(sc.textures) == 1
     meshes = [sc.meshes[sc.objects[o].mesh] for o in objs]
     # model 0: the quad fan-triangulated, uv and normals kept, 4 unique (v, vt, vn)
     m0 = meshes[0]
@@ -215,7 +220,7 @@ def test_load_obj_scene_structure(tmp_path):
     for o in objs:
         np.testing.assert_allclose(sc.objects[o].transform, xf)
         np.testing.assert_allclose(sc.objects[o].inv_transform @ xf, np.eye(4), atol=1e-6)
-        assert sc.objects[o].materials == list(range(6))
+        assert sc.objects[o].materials == list(range(7))
 
 
 def test_load_obj_without_mtl_is_grey(tmp_path):
@@ -265,3 +270,27 @@ def test_imported_cornell_renders_like_builtin(tmp_path):
     assert abs(a.mean() - b.mean()) / a.mean() < 2e-2
     close = np.abs(a - b) <= 1e-3 * np.maximum(1.0, np.abs(a))
     assert close.all(axis=2).mean() > 0.9
+
+
+FIREPLACE = "/root/reference/assets/fireplace_room"
+
+
+@pytest.mark.skipif(not os.path.isdir(FIREPLACE), reason="the reference's fireplace asset is not on this machine")
+def test_fireplace_mtl_and_textures():
+    # The reference's own asset (its OBJ is not shipped): every MTL material
+    # converts, and each map_Kd PNG decodes to the same pixels as OpenCV's
+    # decoder gives.
+    cv2 = pytest.importorskip("cv2")
+    sc = SceneData()
+    mtl = I.parse_mtl(os.path.join(FIREPLACE, "fireplace_room.mtl"))
+    assert len(mtl) == 22
+    kinds = {}
+    for name, m in mtl.items():
+        kinds[name] = sc.materials[sc.add_material(I.convert_material(m, FIREPLACE, sc))].kind
+    assert kinds["grey_and_white_room:BrushedStainlessSteel"] == A.MATERIAL_CONDUCTOR
+    assert kinds["grey_and_white_room:Floor"] == A.MATERIAL_LAMBERTIAN
+    textured = [m for m in mtl.values() if "map_Kd" in m]
+    assert len(sc.textures) == len(textured) > 0
+    for m, img in zip(textured, sc.textures):
+        ref = cv2.imread(os.path.join(FIREPLACE, m["map_Kd"].replace("\\", "/")), cv2.IMREAD_COLOR)[:, :, ::-1]
+        np.testing.assert_array_equal(img, ref)

@@ -394,8 +394,9 @@ __global__ void AR_TRAVERSAL_BOUNDS k_bd_extend(const __grid_constant__ BdParams
         });
 }
 
-// One bounce of both subpaths (:368-434, :498-556).
-__global__ void __launch_bounds__(256) k_bd_vertex(BdParams P, uint32_t depth) {
+// One bounce of both subpaths (:368-434, :498-556).  <= 64 registers, as
+// k_shade: latency-bound, faster at double occupancy despite spills.
+__global__ void __launch_bounds__(256, 4) k_bd_vertex(BdParams P, uint32_t depth) {
     const uint32_t n = P.counts[depth];
     const int b = depth & 1;
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {

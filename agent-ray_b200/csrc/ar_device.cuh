@@ -226,7 +226,7 @@ struct Traverser {
     static constexpr uint32_t kNodeGroup = 0x80000000u, kMarker = 0x40000000u;
     const DevScene* sc;
     Ray world, local;
-    RayPre pre;
+    RayPre pre, wpre;  // wpre: the world ray's (closest hit keeps it to restore on instance exit)
     HitRec hit;
     float ds, best_l, bu, bv;
     uint32_t cur_inst, best_l_slot, node, guard;
@@ -242,6 +242,7 @@ struct Traverser {
         hit.inst = kInvalid;
         hit.u = hit.v = 0.f;
         pre = precompute(r.o, r.d, r.tmin);
+        if (!kAnyHit) wpre = pre;
         in_blas = false;
         ds = 1.f;
         cur_inst = kInvalid;
@@ -342,7 +343,8 @@ struct Traverser {
                     }
                 }
                 in_blas = false;
-                pre = precompute(world.o, world.d, world.tmin);
+                // (any-hit recomputes: keeping the copy costs its kernel more than it saves)
+                pre = kAnyHit ? precompute(world.o, world.d, world.tmin) : wpre;
                 continue;
             }
             // Instance leaf group: enter the next instance.

@@ -328,7 +328,8 @@ def test_textured_same_stream_matches_oracle(ctx, kind, spp):
     assert np.abs(plain - gpu).mean() > 1e-3  # the textures do change the image
 
 
-def test_imported_obj_scene_renders_like_oracle(ctx, tmp_path):
+@pytest.mark.parametrize("kind,spp,frac", [(A.INTEGRATOR_PT, 16, 0.95), (A.INTEGRATOR_BDPT, 8, 0.85)])
+def test_imported_obj_scene_renders_like_oracle(ctx, tmp_path, kind, spp, frac):
     # An OBJ/MTL scene through the importer: a textured floor (map_Kd PNG,
     # tiled uv), a conductor and a glass box, lit by a quad light.
     from agentray import importer as I
@@ -350,13 +351,13 @@ def test_imported_obj_scene_renders_like_oracle(ctx, tmp_path):
     I.load_obj_scene(sc, str(tmp_path / "s.obj"))
     S.add_quad_light(sc, (-0.3, 1.5, -0.3), (0.6, 0.0, 0.0), (0.0, 0.0, 0.6), (10.0, 10.0, 10.0))
     cam = agentray.scene_data.Camera((0.0, 1.0, 2.2), (0.0, 0.2, 0.0), (0.0, 1.0, 0.0), 45.0, 1.0)
-    cfg = integrator_cfg(A.INTEGRATOR_PT, spp=16, max_depth=8, rr_depth=3, seed=9)
+    cfg = integrator_cfg(kind, spp=spp, max_depth=8, rr_depth=3, seed=9)
     gpu = _render_gpu(ctx, sc, cam, cfg, 40, 40)
     ref = O.OracleScene(sc).render(cam, cfg, 40, 40, sampler=O.SAMPLER_COUNTER)
     assert np.isfinite(gpu).all()
     assert abs(gpu.mean() - ref.mean()) / ref.mean() < 1.5e-2
     close = np.abs(gpu - ref) <= 1e-2 * np.maximum(1.0, np.abs(ref))
-    assert close.all(axis=2).mean() >= 0.95, close.all(axis=2).mean()
+    assert close.all(axis=2).mean() >= frac, close.all(axis=2).mean()
 
 
 @pytest.mark.parametrize("h,w", [(37, 29), (1, 1), (256, 200)])
@@ -378,3 +379,17 @@ def test_film_save_exr_matches_oracle_bytes(ctx, tmp_path, h, w):
     want = (tmp_path / "o.exr").read_bytes()
     assert (tmp_path / "g.exr").read_bytes() == want
     assert (tmp_path / "d.exr").read_bytes() == want
+
+
+def test_gdpt_textured_same_stream_matches_oracle(ctx):
+    # GDPT's base/offset path roles shade textured surfaces through the same
+    # kernels: primal and gradient films against the oracle's.
+    sc, cam = S.cornell_box(1, textured=True)
+    cfg = integrator_cfg(A.INTEGRATOR_GDPT, spp=8, max_depth=6, seed=11)
+    w, h = 48, 40
+    gpu = _render_gpu(ctx, sc, cam, cfg, w, h)
+    ref = O.OracleScene(sc).render(cam, cfg, w, h, sampler=O.SAMPLER_COUNTER)
+    assert np.isfinite(gpu).all()
+    assert abs(gpu.mean() - ref.mean()) / ref.mean() < 1e-2
+    close = np.abs(gpu - ref) <= 2e-2 * np.maximum(1.0, np.abs(ref))
+    assert close.all(axis=2).mean() >= 0.95, close.all(axis=2).mean()

@@ -294,3 +294,20 @@ def test_fireplace_mtl_and_textures():
     for m, img in zip(textured, sc.textures):
         ref = cv2.imread(os.path.join(FIREPLACE, m["map_Kd"].replace("\\", "/")), cv2.IMREAD_COLOR)[:, :, ::-1]
         np.testing.assert_array_equal(img, ref)
+
+
+def test_obj_normals_without_uv_and_ignored_statements(tmp_path):
+    # `f v//vn` keeps normals without uv; points, lines, smoothing groups and
+    # degenerate faces (< 3 corners) make no triangles (GPU_LOAD_OPTIONS
+    # ignores points and lines).
+    (tmp_path / "n.obj").write_text(
+        "v 0 0 0\nv 1 0 0\nv 0 1 0\nv 1 1 0\nvn 0 0 1\nvn 0 0 -1\n"
+        "s 1\np 1\nl 1 2\nf 1//1 2//1 3//1\nf 2//2 4//2 3//2\nf 1 2\n")
+    sc = SceneData()
+    objs = I.load_obj_scene(sc, str(tmp_path / "n.obj"))
+    assert len(objs) == 1
+    m = sc.meshes[sc.objects[objs[0]].mesh]
+    assert m.num_triangles == 2 and m.tex_coords is None
+    # vertex 2 and 3 appear with two different normals -> split (single index)
+    assert m.positions.shape[0] == 6 and m.normals.shape == (6, 3)
+    np.testing.assert_array_equal(m.normals[m.indices[1]], np.array([[0, 0, -1]] * 3, np.float32))

@@ -24,6 +24,8 @@ Workloads (seeded synthetic inputs with the stated shapes; no dataset exists):
   pt_cornell  PT Cornell box (34 tris + quad light, 256x256, 16 spp, depth 8);
               one step = one full render.
   pt_cornell_glass  config 1 with rough-glass (DielectricBsdf) objects.
+  pt_cornell_textured  config 1 with checker ImageTextures on the floor and
+              back wall (bilinear, repeat-wrapped uv).
   pt_served4  PT on served scene 4 (139k tris, 335 instances), 512x512, 16 spp.
   bdpt_served4 BDPT on served scene 4, 512x512, 16 spp, depth 8.
   bdpt_room   BDPT on the 200k-tri room, 512x512, 64 spp, depth 10, FP64 film.
@@ -485,6 +487,12 @@ def run_pt_cornell(args, rank, local, world, torch, ctx, barrier, dist, peaks, p
         W = H = 512
         desc = "pt_served4: PT on served scene 4 (138,944 tris, 335 instances, 2 quad lights), 512x512, 16 spp, depth 8"
         prof_name = "pt_extend_served4"
+    elif args.workload == "pt_cornell_textured":
+        sc, cam = S.cornell_box(1, textured=True)
+        W = H = 256
+        desc = ("pt_cornell_textured: PT Cornell box with 16x16 and 7x7 checker ImageTextures (sRGB, bilinear, "
+                "repeat) on floor and back wall, 256x256, 16 spp, depth 8, RR 3")
+        prof_name = "pt_extend_cornell_textured"
     elif args.workload == "pt_cornell_glass":
         sc, cam = S.cornell_box(1, glass=True)
         W = H = 256
@@ -793,7 +801,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="served",
-                    choices=["served", "pt_cornell", "pt_cornell_glass", "pt_served4", "bdpt_served4", "bdpt_room",
+                    choices=["served", "pt_cornell", "pt_cornell_glass", "pt_cornell_textured", "pt_served4",
+                             "bdpt_served4", "bdpt_room",
                              "gdpt_room", "bvh"])
     ap.add_argument("--jobs", type=int, default=2000)
     ap.add_argument("--window-jobs", dest="window_jobs", type=int, default=16)
@@ -833,7 +842,7 @@ def main():
 
     if args.workload == "served":
         run_served(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind)
-    elif args.workload in ("pt_cornell", "pt_cornell_glass", "pt_served4"):
+    elif args.workload in ("pt_cornell", "pt_cornell_glass", "pt_cornell_textured", "pt_served4"):
         run_pt_cornell(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind, stream)
     elif args.workload in ("bdpt_served4", "bdpt_room", "gdpt_room"):
         run_room(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind, stream)

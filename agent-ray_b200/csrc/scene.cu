@@ -366,6 +366,8 @@ void create_scene(ar_context* ctx, const ar_scene_desc* d, ar_scene** out) {
         const ar_texture_desc& td = d->textures[t];
         AR_REQUIRE(td.rgb8 && td.width > 0 && td.height > 0, AR_ERR_INVALID_ARGUMENT, "empty texture");
         AR_REQUIRE(uint64_t(td.width) * td.height < (1ull << 28), AR_ERR_INVALID_ARGUMENT, "texture too large");
+        AR_REQUIRE(texels.size() + uint64_t(td.width) * td.height < (1ull << 31), AR_ERR_INVALID_ARGUMENT,
+                   "textures too large in total (texel offsets are 32-bit)");
         trec[t] = TextureRecord{uint32_t(texels.size()), td.width, td.height, 0};
         const auto lin = [](uint8_t b) {
             const float x = float(b) / 255.0f;

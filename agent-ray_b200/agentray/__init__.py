@@ -131,6 +131,7 @@ class Scene:
         dev = not isinstance(org_tmin, np.ndarray)
         if dev:
             import torch
+            org_tmin, dir_tmax = self._device_rays(org_tmin, dir_tmax)
             hits = torch.empty((org_tmin.shape[0], 4), dtype=torch.float32, device=org_tmin.device)
             inst = torch.empty((org_tmin.shape[0],), dtype=torch.int32, device=org_tmin.device)
             b = self._batch(org_tmin, dir_tmax, True)
@@ -147,7 +148,26 @@ class Scene:
                                      0))
         return hits, inst
 
+    @staticmethod
+    def _device_rays(org_tmin, dir_tmax):
+        """Contiguous float32 (n, 4) CUDA tensors on one device."""
+        import torch
+        if not (isinstance(dir_tmax, torch.Tensor) and org_tmin.is_cuda and dir_tmax.device == org_tmin.device):
+            raise ValueError("org_tmin and dir_tmax must be CUDA tensors on the same device")
+        if org_tmin.dim() != 2 or org_tmin.shape[1] != 4 or dir_tmax.shape != org_tmin.shape:
+            raise ValueError("rays must be (n, 4) arrays")
+        return org_tmin.to(torch.float32).contiguous(), dir_tmax.to(torch.float32).contiguous()
+
     def trace_any(self, org_tmin, dir_tmax):
+        """Occlusion (Scene::occluded) for (n,4) float32 ray arrays (numpy on the
+        host, or torch CUDA tensors).  Returns (n,) uint8: 1 = occluded."""
+        if not isinstance(org_tmin, np.ndarray):
+            import torch
+            org_tmin, dir_tmax = self._device_rays(org_tmin, dir_tmax)
+            occ = torch.empty((org_tmin.shape[0],), dtype=torch.uint8, device=org_tmin.device)
+            b = self._batch(org_tmin, dir_tmax, True)
+            check(lib().ar_trace_any(self.ctx.handle, self.handle, C.byref(b), occ.data_ptr(), 1))
+            return occ
         org_tmin = np.ascontiguousarray(org_tmin, np.float32)
         dir_tmax = np.ascontiguousarray(dir_tmax, np.float32)
         occ = np.empty(org_tmin.shape[0], np.uint8)

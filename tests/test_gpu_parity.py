@@ -393,3 +393,19 @@ def test_gdpt_textured_same_stream_matches_oracle(ctx):
     assert abs(gpu.mean() - ref.mean()) / ref.mean() < 1e-2
     close = np.abs(gpu - ref) <= 2e-2 * np.maximum(1.0, np.abs(ref))
     assert close.all(axis=2).mean() >= 0.95, close.all(axis=2).mean()
+
+
+def test_trace_device_tensors_match_host_arrays(ctx):
+    # Scene.trace_closest / trace_any take torch CUDA tensors (results stay on
+    # the device) as well as host arrays; both give the same answers.
+    import torch
+    soup = S.triangle_soup(5000, seed=8)
+    g = agentray.Scene(ctx, soup)
+    ot, dt = S.soup_rays(4000, seed=9)
+    h_hits, h_inst = g.trace_closest(ot, dt)
+    d_hits, d_inst = g.trace_closest(torch.from_numpy(ot).cuda(), torch.from_numpy(dt).cuda())
+    np.testing.assert_array_equal(d_hits.cpu().numpy().view(np.uint32), h_hits.view(np.uint32))
+    np.testing.assert_array_equal(d_inst.cpu().numpy().view(np.uint32), h_inst.view(np.uint32))
+    h_occ = g.trace_any(ot, dt)
+    d_occ = g.trace_any(torch.from_numpy(ot).cuda().double(), torch.from_numpy(dt).cuda().double())
+    np.testing.assert_array_equal(d_occ.cpu().numpy(), h_occ)

@@ -14,6 +14,7 @@ src/cameras.rs, src/film.rs) maps as follows:
 
 All work runs in the CUDA library; nothing here computes on the CPU.
 """
+import contextlib
 import ctypes as C
 import os
 from dataclasses import dataclass
@@ -36,10 +37,28 @@ class Context:
     def __init__(self, device=0):
         self.device = device
         self.handle = C.c_void_p()
+        self._stream = None  # None: the context's own stream
         check(lib().ar_context_create(device, C.byref(self.handle)))
 
     def set_stream(self, stream_ptr):
-        check(lib().ar_context_set_stream(self.handle, C.c_void_p(stream_ptr)))
+        """Launch on this cudaStream_t (an int); None or 0 restores the
+        context's own stream."""
+        check(lib().ar_context_set_stream(self.handle, C.c_void_p(stream_ptr or None)))
+        self._stream = stream_ptr or None
+
+    @contextlib.contextmanager
+    def on_torch_stream(self, tensor):
+        """Runs the enclosed library calls on torch's current stream of
+        `tensor`'s device, so that they are ordered after the torch work that
+        produced their device inputs and before the torch work that reads
+        their device outputs."""
+        import torch
+        prev = self._stream
+        self.set_stream(torch.cuda.current_stream(tensor.device).cuda_stream)
+        try:
+            yield
+        finally:
+            self.set_stream(prev)
 
     def synchronize(self):
         check(lib().ar_context_synchronize(self.handle))
@@ -135,8 +154,9 @@ class Scene:
             hits = torch.empty((org_tmin.shape[0], 4), dtype=torch.float32, device=org_tmin.device)
             inst = torch.empty((org_tmin.shape[0],), dtype=torch.int32, device=org_tmin.device)
             b = self._batch(org_tmin, dir_tmax, True)
-            check(lib().ar_trace_closest(self.ctx.handle, self.handle, C.byref(b), hits.data_ptr(),
-                                         inst.data_ptr(), 1))
+            with self.ctx.on_torch_stream(org_tmin):
+                check(lib().ar_trace_closest(self.ctx.handle, self.handle, C.byref(b), hits.data_ptr(),
+                                             inst.data_ptr(), 1))
             return hits, inst
         org_tmin = np.ascontiguousarray(org_tmin, np.float32)
         dir_tmax = np.ascontiguousarray(dir_tmax, np.float32)
@@ -166,7 +186,8 @@ class Scene:
             org_tmin, dir_tmax = self._device_rays(org_tmin, dir_tmax)
             occ = torch.empty((org_tmin.shape[0],), dtype=torch.uint8, device=org_tmin.device)
             b = self._batch(org_tmin, dir_tmax, True)
-            check(lib().ar_trace_any(self.ctx.handle, self.handle, C.byref(b), occ.data_ptr(), 1))
+            with self.ctx.on_torch_stream(org_tmin):
+                check(lib().ar_trace_any(self.ctx.handle, self.handle, C.byref(b), occ.data_ptr(), 1))
             return occ
         org_tmin = np.ascontiguousarray(org_tmin, np.float32)
         dir_tmax = np.ascontiguousarray(dir_tmax, np.float32)
@@ -225,8 +246,9 @@ def film_to_rgb8(ctx, hdr, tone_mapper=A.TONEMAP_CLAMP, gamma=2.2, scale=1.0, wh
         hdr = hdr.to(torch.float32).contiguous()
         h, w = hdr.shape[0], hdr.shape[1]
         out = torch.empty((h, w, 3), dtype=torch.uint8, device=hdr.device)
-        check(lib().ar_film_to_rgb8(ctx.handle, hdr.data_ptr(), w, h, tone_mapper, white_point, gamma, scale,
-                                    out.data_ptr(), 1))
+        with ctx.on_torch_stream(hdr):
+            check(lib().ar_film_to_rgb8(ctx.handle, hdr.data_ptr(), w, h, tone_mapper, white_point, gamma, scale,
+                                        out.data_ptr(), 1))
         return out
     x = np.ascontiguousarray(hdr, np.float32)
     h, w = x.shape[0], x.shape[1]
@@ -245,7 +267,8 @@ def film_save_exr(ctx, hdr, path, scale=1.0):
     if not isinstance(hdr, np.ndarray):
         import torch
         x = hdr.to(torch.float32).contiguous()
-        check(lib().ar_film_save_exr(ctx.handle, x.data_ptr(), x.shape[1], x.shape[0], scale, 1, p))
+        with ctx.on_torch_stream(x):
+            check(lib().ar_film_save_exr(ctx.handle, x.data_ptr(), x.shape[1], x.shape[0], scale, 1, p))
         return
     x = np.ascontiguousarray(hdr, np.float32)
     check(lib().ar_film_save_exr(ctx.handle, x.ctypes.data, x.shape[1], x.shape[0], scale, 0, p))
@@ -330,8 +353,9 @@ class _Integrator:
         cfg = self.cfg()
         cam = camera.desc()
         if out is not None and not isinstance(out, np.ndarray):
-            check(lib().ar_render(scene.ctx.handle, scene.handle, C.byref(cam), C.byref(cfg), width, height,
-                                  out.data_ptr(), 1))
+            with scene.ctx.on_torch_stream(out):
+                check(lib().ar_render(scene.ctx.handle, scene.handle, C.byref(cam), C.byref(cfg), width, height,
+                                      out.data_ptr(), 1))
             return out
         buf = np.empty(width * height * 3, np.float32) if out is None else out
         check(lib().ar_render(scene.ctx.handle, scene.handle, C.byref(cam), C.byref(cfg), width, height,

@@ -27,9 +27,13 @@ def render_shard(integrator, scene, camera, width, height, begin, end, out):
     cfg = integrator.cfg()
     cam = camera.desc()
     on_device = not isinstance(out, np.ndarray)
-    ptr = out.data_ptr() if on_device else out.ctypes.data
+    if on_device:
+        with scene.ctx.on_torch_stream(out):
+            check(lib().ar_render_samples(scene.ctx.handle, scene.handle, C.byref(cam), C.byref(cfg), width, height,
+                                          begin, end, out.data_ptr(), 1))
+        return out
     check(lib().ar_render_samples(scene.ctx.handle, scene.handle, C.byref(cam), C.byref(cfg), width, height, begin,
-                                  end, ptr, 1 if on_device else 0))
+                                  end, out.ctypes.data, 0))
     return out
 
 

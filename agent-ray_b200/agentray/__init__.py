@@ -53,8 +53,18 @@ class Context:
         produced their device inputs and before the torch work that reads
         their device outputs."""
         import torch
+        ts = torch.cuda.current_stream(tensor.device)
+        if ts.cuda_stream == 0:
+            # torch's legacy default stream cannot be handed to the library (a
+            # null stream selects the context's own): order by synchronising.
+            ts.synchronize()
+            try:
+                yield
+            finally:
+                self.synchronize()
+            return
         prev = self._stream
-        self.set_stream(torch.cuda.current_stream(tensor.device).cuda_stream)
+        self.set_stream(ts.cuda_stream)
         try:
             yield
         finally:

@@ -225,8 +225,13 @@ template <bool kAnyHit>
 struct Traverser {
     static constexpr uint32_t kNodeGroup = 0x80000000u, kMarker = 0x40000000u;
     const DevScene* sc;
-    Ray world, local;
-    RayPre pre, wpre;  // wpre: the world ray's (closest hit keeps it to restore on instance exit)
+    // World ray: its direction and t_max; its origin and t_min live in wpre
+    // (closest hit, which keeps the world ray's precompute to restore on
+    // instance exit) or in wo/wtmin (any hit, which recomputes it).  Inside an
+    // instance the local ray is pre.o / ld / pre.tmin.
+    f3 wd, wo, ld;
+    float wtmin, wtmax;
+    RayPre pre, wpre;
     HitRec hit;
     float ds, best_l, bu, bv;
     uint32_t cur_inst, best_l_slot, node, guard;
@@ -236,7 +241,12 @@ struct Traverser {
 
     __device__ __forceinline__ void start(const DevScene* s, const Ray& r) {
         sc = s;
-        world = r;
+        wd = r.d;
+        wtmax = r.tmax;
+        if (kAnyHit) {
+            wo = r.o;
+            wtmin = r.tmin;
+        }
         hit.t = r.tmax;
         hit.slot = kInvalid;
         hit.inst = kInvalid;
@@ -273,9 +283,9 @@ struct Traverser {
                         tbits &= tbits - 1;
                         const TriRecord tr = load_tri(sc->tris, tbase + b);
                         float t, u, v;
-                        if (tri_test(tr, local.o, local.d, local.tmin, best_l, t, u, v) && t < best_l) {
+                        if (tri_test(tr, pre.o, ld, pre.tmin, best_l, t, u, v) && t < best_l) {
                             if (kAnyHit) {
-                                if (__fdiv_rn(t, ds) < world.tmax) {
+                                if (__fdiv_rn(t, ds) < wtmax) {
                                     hit.t = t;
                                     hit.slot = tbase + b;
                                     hit.inst = cur_inst;
@@ -344,7 +354,7 @@ struct Traverser {
                 }
                 in_blas = false;
                 // (any-hit recomputes: keeping the copy costs its kernel more than it saves)
-                pre = kAnyHit ? precompute(world.o, world.d, world.tmin) : wpre;
+                pre = kAnyHit ? precompute(wo, wd, wtmin) : wpre;
                 continue;
             }
             // Instance leaf group: enter the next instance.
@@ -360,20 +370,19 @@ struct Traverser {
             const f3 c0 = mk(m0.x, m0.y, m0.z), c1 = mk(m0.w, m1.x, m1.y), c2 = mk(m1.z, m1.w, m2.x),
                      c3 = mk(m2.y, m2.z, m2.w);
             // glam transform_point3a / transform_vector3a: ((c0*x + c1*y) + c2*z) + c3
-            const f3 lo =
-                add_rn(c3, add_rn(add_rn(scale_rn(c0, world.o.x), scale_rn(c1, world.o.y)), scale_rn(c2, world.o.z)));
-            const f3 ldu = add_rn(add_rn(scale_rn(c0, world.d.x), scale_rn(c1, world.d.y)), scale_rn(c2, world.d.z));
+            const f3 w_o = kAnyHit ? wo : wpre.o;
+            const f3 lo = add_rn(c3, add_rn(add_rn(scale_rn(c0, w_o.x), scale_rn(c1, w_o.y)), scale_rn(c2, w_o.z)));
+            const f3 ldu = add_rn(add_rn(scale_rn(c0, wd.x), scale_rn(c1, wd.y)), scale_rn(c2, wd.z));
             const float scale = __fsqrt_rn(dot_rn(ldu, ldu));
             if (scale < FLT_EPSILON) continue;
             ds = scale;
-            local.o = lo;
-            local.d = normalize_rn(ldu);
-            local.tmin = __fmul_rn(world.tmin, ds);
-            best_l = __fmul_rn(kAnyHit ? world.tmax : hit.t, ds);
+            ld = normalize_rn(ldu);
+            const float ltmin = __fmul_rn(kAnyHit ? wtmin : wpre.tmin, ds);
+            best_l = __fmul_rn(kAnyHit ? wtmax : hit.t, ds);
             best_l_slot = kInvalid;
             cur_inst = m3.y;
             in_blas = true;
-            pre = precompute(local.o, local.d, local.tmin);
+            pre = precompute(lo, ld, ltmin);
             if (sp >= kTraversalStack) { atomicExch(err, 1); return true; }
             stack[sp++] = make_uint2(0, kMarker);
             node = m3.x;

@@ -143,7 +143,9 @@ __device__ __forceinline__ RayPre precompute(f3 o, f3 d, float tmin) {
     r.inv.x = __frcp_rn(fabsf(d.x) > eps ? d.x : copysignf(eps, d.x));
     r.inv.y = __frcp_rn(fabsf(d.y) > eps ? d.y : copysignf(eps, d.y));
     r.inv.z = __frcp_rn(fabsf(d.z) > eps ? d.z : copysignf(eps, d.z));
-    r.oct = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
+    // the octant follows the reciprocal's sign, -0.0 included (its reciprocal
+    // is -1e20): near and far planes must swap exactly when inv is negative
+    r.oct = (signbit(d.x) ? 1u : 0u) | (signbit(d.y) ? 2u : 0u) | (signbit(d.z) ? 4u : 0u);
     r.tmin = tmin;
     return r;
 }

@@ -69,8 +69,13 @@ def test_any_hit_soup(ctx):
     ref = osc.trace_any(ot, dt)
     mism = occ != ref
     if mism.any():
+        # excused only by a boundary case on the side that reports occlusion:
+        # its hit lies within 1e-6 of a triangle edge or of t_max
         r = osc.trace_closest(ot[mism], dt[mism])
-        assert np.all(_edge_case(r["u"], r["v"]) | (np.abs(r["t"] - 0.25) < 1e-6)), f"{mism.sum()} mismatches"
+        gh, _ = g.trace_closest(ot[mism], dt[mism])
+        near = lambda t, u, v: _edge_case(u, v) | (np.abs(t - 0.25) < 1e-6)
+        ok = np.where(ref[mism] != 0, near(r["t"], r["u"], r["v"]), near(gh[:, 0], gh[:, 1], gh[:, 2]))
+        assert np.all(ok), f"{(~ok).sum()} unexcused of {mism.sum()} mismatches"
     assert (occ == ref).mean() > 0.9999
 
 

@@ -5,8 +5,11 @@ seeded inputs.  Bars:
     (|t_gpu - t_ref| <= 1e-6 * max(1, t)) or hits within 1e-6 of a triangle edge
     in barycentric terms.  Any-hit booleans likewise.
   * Images: same counter-based sample stream -> per-pixel agreement (rel. 1e-3)
-    on >= 98% of pixels and mean within 0.5%; an independent-seed run must
-    pass a per-pixel z-test (|z| > 4 on at most 0.5% of pixels).
+    on >= 99.5% of pixels and means within 1e-4 (PT, BDPT, GDPT, textures;
+    measured: every pixel); through glass, where an ulp of CUDA's cosf/sqrtf
+    can bend a path elsewhere, rel. 1e-2 on >= 98% (PT) / 85% (BDPT); an
+    independent-seed run must pass a per-pixel z-test (|z| > 4 on at most
+    0.5% of pixels).
   * Red-black SOR: bit-exact to the oracle.
   * Film output: 8-bit bytes equal up to 1 LSB on < 0.1% (CUDA vs libm powf);
     EXR files byte-identical.
@@ -138,8 +141,8 @@ def test_pt_same_stream_matches_oracle(ctx, point_light):
     gpu = _render_gpu(ctx, sc, cam, cfg, w, h)
     ref = O.OracleScene(sc).render(cam, cfg, w, h, sampler=O.SAMPLER_COUNTER)
     close = np.abs(gpu - ref) <= 1e-3 * np.maximum(1.0, np.abs(ref))
-    assert close.all(axis=2).mean() >= 0.98, close.all(axis=2).mean()
-    assert abs(gpu.mean() - ref.mean()) / ref.mean() < 5e-3
+    assert close.all(axis=2).mean() >= 0.995, close.all(axis=2).mean()
+    assert abs(gpu.mean() - ref.mean()) / ref.mean() < 1e-4
 
 
 def welch_fail_fraction(a_reps, b_reps, thresh=4.5):
@@ -211,9 +214,9 @@ def test_gdpt_same_stream_matches_oracle(ctx):
     w, h = 48, 40
     gpu = _render_gpu(ctx, sc, cam, cfg, w, h)
     ref = O.OracleScene(sc).render(cam, cfg, w, h, sampler=O.SAMPLER_COUNTER)
-    assert abs(gpu.mean() - ref.mean()) / ref.mean() < 1e-2
-    close = np.abs(gpu - ref) <= 2e-2 * np.maximum(1.0, np.abs(ref))
-    assert close.all(axis=2).mean() >= 0.95
+    assert abs(gpu.mean() - ref.mean()) / ref.mean() < 1e-4
+    close = np.abs(gpu - ref) <= 1e-3 * np.maximum(1.0, np.abs(ref))
+    assert close.all(axis=2).mean() >= 0.995
 
 
 @pytest.mark.parametrize("point_light", [True, False])
@@ -223,9 +226,9 @@ def test_bdpt_same_stream_matches_oracle(ctx, point_light):
     w = h = 48
     gpu = _render_gpu(ctx, sc, cam, cfg, w, h)
     ref = O.OracleScene(sc).render(cam, cfg, w, h, sampler=O.SAMPLER_COUNTER)
-    assert abs(gpu.mean() - ref.mean()) / ref.mean() < 1e-2
-    close = np.abs(gpu - ref) <= 1e-2 * np.maximum(1.0, np.abs(ref))
-    assert close.all(axis=2).mean() >= 0.95, close.all(axis=2).mean()
+    assert abs(gpu.mean() - ref.mean()) / ref.mean() < 1e-4
+    close = np.abs(gpu - ref) <= 1e-3 * np.maximum(1.0, np.abs(ref))
+    assert close.all(axis=2).mean() >= 0.995, close.all(axis=2).mean()
 
 
 def test_bdpt_statistically_equal_to_independent_oracle(ctx):
@@ -275,7 +278,7 @@ def test_film_to_rgb8_matches_oracle(ctx, tm, wp):
 # connects every vertex of both subpaths, so fewer pixels agree exactly than
 # without glass (~0.90 vs 1.00 for BDPT; measured); the bias bar stays (mean
 # within 1.5%) and the independent-seed test below shows no bias.
-@pytest.mark.parametrize("kind,spp,frac", [(A.INTEGRATOR_PT, 16, 0.95), (A.INTEGRATOR_BDPT, 8, 0.85)])
+@pytest.mark.parametrize("kind,spp,frac", [(A.INTEGRATOR_PT, 16, 0.98), (A.INTEGRATOR_BDPT, 8, 0.85)])
 def test_dielectric_same_stream_matches_oracle(ctx, kind, spp, frac):
     # DielectricBsdf (rough GGX glass): refraction, total internal reflection
     # and the reference's face-forwarded frame (wo.z > 0, so eta is always the
@@ -334,8 +337,8 @@ def test_textured_same_stream_matches_oracle(ctx, kind, spp):
     gpu = _render_gpu(ctx, sc, cam, cfg, w, h)
     ref = O.OracleScene(sc).render(cam, cfg, w, h, sampler=O.SAMPLER_COUNTER)
     close = np.abs(gpu - ref) <= 1e-3 * np.maximum(1.0, np.abs(ref))
-    assert close.all(axis=2).mean() >= 0.98, close.all(axis=2).mean()
-    assert abs(gpu.mean() - ref.mean()) / ref.mean() < 5e-3
+    assert close.all(axis=2).mean() >= 0.995, close.all(axis=2).mean()
+    assert abs(gpu.mean() - ref.mean()) / ref.mean() < 1e-4
     plain = _render_gpu(ctx, S.cornell_box(1)[0], cam, cfg, w, h)
     assert np.abs(plain - gpu).mean() > 1e-3  # the textures do change the image
 
@@ -402,9 +405,9 @@ def test_gdpt_textured_same_stream_matches_oracle(ctx):
     gpu = _render_gpu(ctx, sc, cam, cfg, w, h)
     ref = O.OracleScene(sc).render(cam, cfg, w, h, sampler=O.SAMPLER_COUNTER)
     assert np.isfinite(gpu).all()
-    assert abs(gpu.mean() - ref.mean()) / ref.mean() < 1e-2
-    close = np.abs(gpu - ref) <= 2e-2 * np.maximum(1.0, np.abs(ref))
-    assert close.all(axis=2).mean() >= 0.95, close.all(axis=2).mean()
+    assert abs(gpu.mean() - ref.mean()) / ref.mean() < 1e-4
+    close = np.abs(gpu - ref) <= 1e-3 * np.maximum(1.0, np.abs(ref))
+    assert close.all(axis=2).mean() >= 0.995, close.all(axis=2).mean()
 
 
 def test_trace_device_tensors_match_host_arrays(ctx):

@@ -173,7 +173,15 @@ void build_scene_accel(ar_scene* s, const ar_accel_opts* o) {
     uint32_t tlas_root = kInvalid, tlas_depth = 0;
     uint64_t tlas_nodes = 0;
     if (!inst_boxes.empty()) {
-        WideBuild tb = build_wide_bvh(inst_boxes, bo);
+        // Single-instance TLAS leaves: a hit TLAS leaf group is pushed on the
+        // traversal stack with its instance mask in the entry's flag word,
+        // whose top two bits mark node groups and instance exits, so a node's
+        // instance mask must stay below bit 30 (8 leaves of up to 4 would
+        // reach bit 31).  One instance per leaf also tests every instance's
+        // own box in its parent's 8-wide node test (measured no slower).
+        BuildOptions tbo = bo;
+        tbo.max_leaf = 1;
+        WideBuild tb = build_wide_bvh(inst_boxes, tbo);
         const uint32_t node_off = uint32_t(nodes.size());
         for (auto n : tb.nodes) {
             n.child_base += node_off;

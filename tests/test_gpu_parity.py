@@ -82,9 +82,14 @@ def test_any_hit_soup(ctx):
     assert (occ == ref).mean() > 0.9999
 
 
-def test_closest_hit_instanced_room(ctx):
+@pytest.mark.parametrize("opts", [None, dict(max_leaf_size=4, sah_node_cost=8.0)])
+def test_closest_hit_instanced_room(ctx, opts):
+    # opts: the default build, and the largest leaves the API allows (4
+    # triangles, node cost 8 so that the SAH keeps full leaves).
     sc, cam = S.room(seed=4, sphere_levels=(3, 3, 2, 2), n_boxes=120)
     g = agentray.Scene(ctx, sc)
+    if opts:
+        g.rebuild(**opts)
     osc = O.OracleScene(sc)
     rng = np.random.default_rng(9)
     n = 100_000

@@ -214,7 +214,7 @@ typedef struct ar_hit {
 } ar_hit;
 
 typedef struct ar_accel_opts {
-    uint32_t max_leaf_size;          /* 1..4 triangles per wide-BVH leaf (default 3) */
+    uint32_t max_leaf_size;          /* 1..4 triangles per BLAS leaf (default 3); TLAS leaves hold one instance */
     uint32_t sah_bins;               /* binned SAH bins (default 32) */
     uint32_t build_threads;          /* host threads for the build (0 = all cores) */
     uint32_t bvh_width;              /* children per node, 2..8 (0 = 8); the node format is 8-wide */

@@ -47,6 +47,7 @@ import json
 import os
 import statistics
 import subprocess
+import tempfile
 import sys
 import threading
 import time
@@ -96,7 +97,10 @@ class ClockSampler:
     def __init__(self, device):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{device}_{os.getpid()}.csv")
+        # raw samples go to $AR_CLOCK_LOG_DIR (default: the system temp dir);
+        # the JSON line carries their summary
+        log_dir = os.environ.get("AR_CLOCK_LOG_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(log_dir, f"clocks_{device}_{os.getpid()}.csv")
 
     def __enter__(self):
         os.makedirs(os.path.dirname(self.path), exist_ok=True)

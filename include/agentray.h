@@ -113,7 +113,8 @@ typedef struct ar_texture_desc {
 
 enum ar_light_kind {
     AR_LIGHT_POINT = 0,              /* src/lights/point.rs */
-    AR_LIGHT_QUAD = 1                /* one-sided quad area light (extension, see DESIGN) */
+    AR_LIGHT_QUAD = 1                /* one-sided quad area light {corner, edge1, edge2, radiance}: an
+                                        extension the configs need (the crate has point lights only) */
 };
 
 typedef struct ar_light_desc {

@@ -1,7 +1,8 @@
 """ctypes binding of the CPU restatement oracle (oracle/_build/liboracle_agentray.so).
 
 TEST INFRASTRUCTURE ONLY.  Imported by tests/, __graft_entry__.smoke() and the
-CPU-baseline leg of bench.py as the checker; never by the product path.
+CPU-baseline / reference legs of bench.py, to check and to time against; never
+by the product path.
 
 PARITY UNPINNED: agent-ray is Rust, has no tests or golden vectors, and cannot
 be built here; the oracle is a line-by-line C++ restatement (see ar_*.hpp).

@@ -118,14 +118,17 @@ def test_empty_and_degenerate_rays(ctx):
     ot, dt = S.soup_rays(5000, seed=4)
     dt[:2500, :3] = np.eye(3, dtype=np.float32)[np.arange(2500) % 3] * np.where(np.arange(2500) % 2, 1, -1)[:, None]
     dt[4000:, 3] = 1e-5
+    dt[3900:4000, :3] = 0.0  # zero directions: Ray::new gives NaN, which hits nothing
     assert (np.signbit(dt[:2500, :3]) & (dt[:2500, :3] == 0)).any()  # -0.0 components included
     hits, inst = g.trace_closest(ot, dt)
     ref = osc.trace_closest(ot, dt)
     same, bad = _compare_hits(hits, inst, ref)
     assert bad.sum() == 0, f"{bad.sum()} mismatches"
     assert same[:2500].mean() > 0.999
-    assert np.all(hits[4000:, 3].view(np.uint32) == INVALID)
+    assert np.all(hits[3900:, 3].view(np.uint32) == INVALID)
+    assert np.all(ref["prim"][3900:4000] == INVALID)
     occ = g.trace_any(ot, dt)
+    assert not occ[3900:4000].any()
     assert (occ == osc.trace_any(ot, dt)).mean() > 0.999
 
 

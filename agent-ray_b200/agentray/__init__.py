@@ -408,6 +408,11 @@ class Server:
         on_device = out is not None and not isinstance(out, np.ndarray)
         if out is None:
             out = np.empty(width * height * 3, np.float32)
+        if on_device:
+            # the server writes `out` from its own streams: let the torch work
+            # queued on this memory finish first
+            import torch
+            torch.cuda.current_stream(out.device).synchronize()
         ptr = out.data_ptr() if on_device else out.ctypes.data
         cam = camera.desc()
         cfg = integrator.cfg()

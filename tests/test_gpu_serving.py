@@ -96,3 +96,23 @@ def test_server_results_match_plain_path_f32(ctx):
     out = srv.result(jid)
     srv.close()
     np.testing.assert_allclose(out, ref, rtol=1e-4, atol=1e-5)
+
+
+def test_device_outputs_match_host_outputs(ctx):
+    # Server.submit(out=<CUDA tensor>) keeps the image on the GPU; it is the
+    # same image as the host-buffer path (f64 films: atomic order only).
+    import torch
+    cb, cam = S.cornell_box(1)
+    scene = agentray.Scene(ctx, cb)
+    srv = agentray.Server(ctx, path_capacity=1 << 18, bdpt_batch_samples=1 << 14)
+    jobs = [(_pt(8, seed=31), 64, 48), (_bdpt(4, seed=32), 48, 40)]
+    host = [srv.submit(scene, cam, integ, w, h) for integ, w, h in jobs]
+    outs = [torch.full((w * h * 3,), float("nan"), dtype=torch.float32, device="cuda") for _, w, h in jobs]
+    dev = [srv.submit(scene, cam, integ, w, h, out=o) for (integ, w, h), o in zip(jobs, outs)]
+    for jid in host + dev:
+        assert srv.wait(jid)["status"] == "done"
+    for (integ, w, h), hj, dj in zip(jobs, host, dev):
+        d = srv.result(dj).cpu().numpy().reshape(h, w, 3)
+        assert np.isfinite(d).all()
+        np.testing.assert_allclose(d, srv.result(hj), rtol=1e-5, atol=1e-6)
+    srv.close()

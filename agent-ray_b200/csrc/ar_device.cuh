@@ -276,7 +276,7 @@ struct Traverser {
         if (++guard > (1u << 22)) { atomicExch(err, 3); return true; }
         if (visit) {
             uint32_t cb, nbits, tbase, tbits;
-            intersect_node(sc->nodes, node, pre, in_blas ? best_l : hit.t, cb, nbits, tbase, tbits);
+            intersect_node(sc->nodes, node, pre, in_blas ? best_l : (kAnyHit ? wtmax : hit.t), cb, nbits, tbase, tbits);
             group = make_uint2(cb, nbits | kNodeGroup);
             if (tbits) {
                 if (in_blas) {

@@ -11,8 +11,11 @@ src/cameras.rs, src/film.rs) maps as follows:
   Integrator::render(&scene, &camera, w, h)    -> integrator.render(scene, camera, w, h) -> Film
   Film::to_hdr_vec()                           -> Film.to_hdr_vec()  ((H*W, 3) float32)
   Scene::intersect / occluded (ray batches)    -> Scene.trace_closest / Scene.trace_any
+  Film::to_rgb_image / save_exr                -> Film.to_rgb_image / save_png / save_exr
+  load_obj_scene(path, transform)              -> importer.load_obj_scene(scene_data, path, transform)
 
-All work runs in the CUDA library; nothing here computes on the CPU.
+Rendering, tracing and film output run in the CUDA library; on the host there
+is only I/O (OBJ/MTL/PNG reading, PNG writing) and descriptor assembly.
 """
 import contextlib
 import ctypes as C
@@ -28,7 +31,7 @@ from .scene_data import Camera, Light, Material, Mesh, Object, SceneData, integr
 __all__ = ["Context", "Scene", "Camera", "Film", "PathTracer", "PathTracerConfig", "BidirectionalPathTracer",
            "BdptConfig", "GradientDomainPathTracer", "GdptConfig", "SceneData", "Mesh", "Object", "Material",
            "Light", "AgentRayError", "integrator_cfg", "lib", "Server", "poisson_reconstruct", "film_to_rgb8",
-           "write_png"]
+           "film_save_exr", "write_png"]
 
 
 class Context:

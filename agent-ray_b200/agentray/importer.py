@@ -173,6 +173,9 @@ def _models(path):
         elif key == "f":
             corners = []
             for a in args:
+                if "/" not in a:  # position only
+                    corners.append((idx(a, len(v)), -1, -1))
+                    continue
                 p = a.split("/")
                 corners.append((idx(p[0], len(v)), idx(p[1], len(vt)) if len(p) > 1 and p[1] else -1,
                                 idx(p[2], len(vn)) if len(p) > 2 and p[2] else -1))
@@ -205,26 +208,28 @@ def load_obj_scene(scene, path, transform=None):
     inv = np.linalg.inv(xf.astype(np.float64)).astype(np.float32)
     objects = []
     for mdl in models:
-        remap, pos, uv, nrm, tris = {}, [], [], [], []
-        has_uv = all(c[1] >= 0 for f in mdl["faces"] for c in f) and len(vt) > 0
-        has_n = all(c[2] >= 0 for f in mdl["faces"] for c in f) and len(vn) > 0
-        for f in mdl["faces"]:
-            tri = []
-            for c in f:
-                key = (c[0], c[1] if has_uv else -1, c[2] if has_n else -1)
-                if key not in remap:  # single index per (v, vt, vn)
-                    remap[key] = len(pos)
-                    pos.append(v[c[0]])
-                    if has_uv:
-                        uv.append(vt[c[1]])
-                    if has_n:
-                        nrm.append(vn[c[2]])
-                tri.append(remap[key])
-            tris.append(tri)
+        c = np.asarray(mdl["faces"], np.int64).reshape(-1, 3)  # corners: (v, vt, vn), -1 = absent
+        has_uv = len(vt) > 0 and bool((c[:, 1] >= 0).all())
+        has_n = len(vn) > 0 and bool((c[:, 2] >= 0).all())
+        key = c.copy()
+        if not has_uv:
+            key[:, 1] = -1
+        if not has_n:
+            key[:, 2] = -1
+        # single index per distinct (v, vt, vn), numbered in order of first use
+        uniq, first, inverse = np.unique(key, axis=0, return_index=True, return_inverse=True)
+        order = np.argsort(first, kind="stable")
+        rank = np.empty(len(order), np.int64)
+        rank[order] = np.arange(len(order))
+        tris = rank[inverse.reshape(-1)].reshape(-1, 3)
+        corner = uniq[order]
+        pos = v[corner[:, 0]]
+        uv = vt[corner[:, 1]] if has_uv else None
+        nrm = vn[corner[:, 2]] if has_n else None
         slot = names.index(mdl["mat"]) if mdl["mat"] in names else 0
-        mesh = Mesh(np.array(pos, np.float32), np.array(tris, np.uint32),
-                    normals=np.array(nrm, np.float32) if has_n else None,
+        mesh = Mesh(np.ascontiguousarray(pos, np.float32), tris.astype(np.uint32),
+                    normals=None if nrm is None else np.ascontiguousarray(nrm, np.float32),
                     material_slots=np.array([slot], np.uint32),
-                    tex_coords=np.array(uv, np.float32) if has_uv else None)
+                    tex_coords=None if uv is None else np.ascontiguousarray(uv, np.float32))
         objects.append(scene.add_object(Object(scene.add_mesh(mesh), list(mat_ids), xf, inv)))
     return objects

@@ -9,9 +9,9 @@ and material) and converts each MTL material to a BSDF:
   map_Kd that loads       -> Lambertian with the ImageTexture
   otherwise               -> Lambertian(Kd, default 0.5)
 with alpha = sqrt(2 / (Ns + 2)) clamped to [1e-3, 1].  Without an MTL every
-model gets one grey Lambertian.  Textures decode here from PNG (8-bit gray,
-gray+alpha, RGB or RGBA, non-interlaced); other formats fall back to Kd, as
-the reference falls back when `image::open` fails.
+model gets one grey Lambertian.  Textures decode here from PNG (every colour
+type, bit depth and interlace mode); other formats fall back to Kd, as the
+reference falls back when `image::open` fails.
 """
 import os
 import struct
@@ -24,39 +24,27 @@ from .scene_data import Material, Mesh, Object
 
 
 # ------------------------------------------------------------------- PNG --
-def read_png(path):
-    """Decodes an 8-bit non-interlaced PNG to an (H, W, 3) uint8 RGB array."""
-    data = open(path, "rb").read()
-    if data[:8] != b"\x89PNG\r\n\x1a\n":
-        raise ValueError("not a PNG file")
-    pos, idat, hdr = 8, [], None
-    while pos < len(data):
-        n = struct.unpack(">I", data[pos:pos + 4])[0]
-        tag = data[pos + 4:pos + 8]
-        body = data[pos + 8:pos + 8 + n]
-        if tag == b"IHDR":
-            hdr = struct.unpack(">IIBBBBB", body)
-        elif tag == b"IDAT":
-            idat.append(body)
-        elif tag == b"IEND":
-            break
-        pos += 12 + n
-    if hdr is None:
-        raise ValueError("PNG without IHDR")
-    w, h, depth, ctype, _, _, interlace = hdr
-    channels = {0: 1, 2: 3, 4: 2, 6: 4}.get(ctype)
-    if depth != 8 or channels is None or interlace != 0:
-        raise ValueError(f"unsupported PNG (depth {depth}, colour type {ctype}, interlace {interlace})")
-    raw = zlib.decompress(b"".join(idat))
-    stride = w * channels
-    out = np.zeros((h, stride), np.uint8)
+_ADAM7 = ((0, 0, 8, 8), (4, 0, 8, 8), (0, 4, 4, 8), (2, 0, 4, 4), (0, 2, 2, 4), (1, 0, 2, 2), (0, 1, 1, 2))
+
+
+def _unfilter(raw, pos, rows, stride, bpp):
+    """Reverses the PNG row filters of `rows` rows of `stride` bytes starting
+    at raw[pos]; bpp = bytes per complete pixel (at least 1).  Returns the
+    (rows, stride) uint8 array and the position after the last row."""
+    out = np.zeros((rows, stride), np.uint8)
     prev = np.zeros(stride, np.int32)
-    for y in range(h):
-        f = raw[y * (stride + 1)]
-        line = np.frombuffer(raw, np.uint8, stride, y * (stride + 1) + 1).astype(np.int32)
+    for y in range(rows):
+        f = raw[pos]
+        line = np.frombuffer(raw, np.uint8, stride, pos + 1).astype(np.int32)
+        pos += stride + 1
         if f in (0, 1, 2):  # none / sub / up reconstruct without a scalar loop
             if f == 1:
-                cur = np.cumsum(line.reshape(w, channels), axis=0).reshape(stride) & 0xFF
+                if stride % bpp == 0:
+                    cur = np.cumsum(line.reshape(-1, bpp), axis=0).reshape(stride) & 0xFF
+                else:
+                    cur = line.copy()
+                    for x in range(bpp, stride):
+                        cur[x] = (cur[x] + cur[x - bpp]) & 0xFF
             else:
                 cur = (line + (prev if f == 2 else 0)) & 0xFF
             out[y] = cur
@@ -66,12 +54,12 @@ def read_png(path):
         # loop over Python ints (several times faster than numpy scalars)
         ln, up, cur = line.tolist(), prev.tolist(), [0] * stride
         for x in range(stride):
-            a = cur[x - channels] if x >= channels else 0
+            a = cur[x - bpp] if x >= bpp else 0
             b = up[x]
             if f == 3:
                 p = (a + b) >> 1
             elif f == 4:
-                c = up[x - channels] if x >= channels else 0
+                c = up[x - bpp] if x >= bpp else 0
                 pa, pb, pc = abs(b - c), abs(a - c), abs(a + b - 2 * c)
                 p = a if pa <= pb and pa <= pc else (b if pb <= pc else c)
             else:
@@ -80,11 +68,79 @@ def read_png(path):
         cur = np.array(cur, np.int32)
         out[y] = cur
         prev = cur
-    px = out.reshape(h, w, channels)
-    if channels == 1:
-        return np.repeat(px, 3, axis=2)
-    if channels == 2:
-        return np.repeat(px[:, :, :1], 3, axis=2)
+    return out, pos
+
+
+def _samples(rows, w, channels, depth):
+    """Unpacked samples (h, w, channels) of unfiltered rows (uint16 for depth 16)."""
+    h = rows.shape[0]
+    if depth == 8:
+        return rows[:, :w * channels].reshape(h, w, channels)
+    if depth == 16:
+        return (rows[:, :2 * w * channels].astype(np.uint16).reshape(h, w * channels, 2) *
+                np.array([256, 1], np.uint16)).sum(axis=2, dtype=np.uint16).reshape(h, w, channels)
+    bits = np.unpackbits(rows, axis=1)[:, :w * channels * depth].reshape(h, w * channels, depth)
+    weights = (1 << np.arange(depth - 1, -1, -1)).astype(np.uint8)
+    return (bits * weights).sum(axis=2, dtype=np.uint8).reshape(h, w, channels)
+
+
+def read_png(path):
+    """Decodes a PNG (grey, grey+alpha, RGB, RGBA or palette; 1-16 bits per
+    sample; plain or Adam7-interlaced) to an (H, W, 3) uint8 RGB array, as
+    ImageTexture::load's `image::open(..).into_rgb8()` does: alpha dropped,
+    grey replicated, sub-8-bit grey scaled to 0..255, 16-bit samples rounded
+    to the nearest 8-bit value (v / 257)."""
+    data = open(path, "rb").read()
+    if data[:8] != b"\x89PNG\r\n\x1a\n":
+        raise ValueError("not a PNG file")
+    pos, idat, hdr, plte = 8, [], None, None
+    while pos + 8 <= len(data):
+        n = struct.unpack(">I", data[pos:pos + 4])[0]
+        tag = data[pos + 4:pos + 8]
+        body = data[pos + 8:pos + 8 + n]
+        if tag == b"IHDR":
+            hdr = struct.unpack(">IIBBBBB", body)
+        elif tag == b"PLTE":
+            plte = np.frombuffer(body, np.uint8).reshape(-1, 3)
+        elif tag == b"IDAT":
+            idat.append(body)
+        elif tag == b"IEND":
+            break
+        pos += 12 + n
+    if hdr is None:
+        raise ValueError("PNG without IHDR")
+    w, h, depth, ctype, _, _, interlace = hdr
+    channels = {0: 1, 2: 3, 3: 1, 4: 2, 6: 4}.get(ctype)
+    allowed = {0: (1, 2, 4, 8, 16), 2: (8, 16), 3: (1, 2, 4, 8), 4: (8, 16), 6: (8, 16)}
+    if channels is None or depth not in allowed[ctype] or interlace not in (0, 1) or w == 0 or h == 0:
+        raise ValueError(f"unsupported PNG (depth {depth}, colour type {ctype}, interlace {interlace})")
+    if ctype == 3 and plte is None:
+        raise ValueError("palette PNG without PLTE")
+    raw = zlib.decompress(b"".join(idat))
+    bpp = max(1, channels * depth // 8)
+    if interlace == 0:
+        rows, _ = _unfilter(raw, 0, h, (w * channels * depth + 7) // 8, bpp)
+        px = _samples(rows, w, channels, depth)
+    else:  # Adam7: seven sub-images, each filtered on its own
+        px = np.zeros((h, w, channels), np.uint16 if depth == 16 else np.uint8)
+        pos = 0
+        for x0, y0, dx, dy in _ADAM7:
+            pw, ph = (w - x0 + dx - 1) // dx, (h - y0 + dy - 1) // dy
+            if pw <= 0 or ph <= 0:
+                continue
+            rows, pos = _unfilter(raw, pos, ph, (pw * channels * depth + 7) // 8, bpp)
+            px[y0::dy, x0::dx] = _samples(rows, pw, channels, depth)
+    if ctype == 3:
+        idx = px[:, :, 0].astype(np.int64)
+        if idx.max() >= plte.shape[0]:
+            raise ValueError("palette index out of range")
+        return np.ascontiguousarray(plte[idx])
+    if depth == 16:
+        px = ((px.astype(np.uint32) * 255 + 32767) // 65535).astype(np.uint8)
+    elif depth < 8:
+        px = (px.astype(np.uint16) * 255 // ((1 << depth) - 1)).astype(np.uint8)
+    if channels <= 2:
+        return np.ascontiguousarray(np.repeat(px[:, :, :1], 3, axis=2))
     return np.ascontiguousarray(px[:, :, :3])
 
 

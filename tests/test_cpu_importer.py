@@ -311,3 +311,72 @@ def test_obj_normals_without_uv_and_ignored_statements(tmp_path):
     # vertex 2 and 3 appear with two different normals -> split (single index)
     assert m.positions.shape[0] == 6 and m.normals.shape == (6, 3)
     np.testing.assert_array_equal(m.normals[m.indices[1]], np.array([[0, 0, -1]] * 3, np.float32))
+
+
+_ADAM7 = ((0, 0, 8, 8), (4, 0, 8, 8), (0, 4, 4, 8), (2, 0, 4, 4), (0, 2, 2, 4), (1, 0, 2, 2), (0, 1, 1, 2))
+
+
+def _pack_rows(samples, depth):
+    """(h, w, c) integer samples -> list of packed scanline bytes (big-endian)."""
+    h = samples.shape[0]
+    flat = samples.reshape(h, -1).astype(np.uint32)
+    if depth == 16:
+        return [np.stack([r >> 8, r & 0xFF], 1).astype(np.uint8).tobytes() for r in flat]
+    if depth == 8:
+        return [r.astype(np.uint8).tobytes() for r in flat]
+    out = []
+    for r in flat:
+        bits = ((r[:, None] >> np.arange(depth - 1, -1, -1)) & 1).astype(np.uint8).reshape(-1)
+        out.append(np.packbits(bits).tobytes())
+    return out
+
+
+def _png_generic(samples, ctype, depth, palette=None, interlace=False):
+    h, w = samples.shape[:2]
+    if interlace:
+        body = b""
+        for x0, y0, dx, dy in _ADAM7:
+            sub = samples[y0::dy, x0::dx]
+            if sub.shape[0] and sub.shape[1]:
+                body += b"".join(b"\0" + r for r in _pack_rows(sub, depth))
+    else:
+        body = b"".join(b"\0" + r for r in _pack_rows(samples, depth))
+
+    def chunk(tag, data):
+        return struct.pack(">I", len(data)) + tag + data + struct.pack(">I", zlib.crc32(tag + data) & 0xFFFFFFFF)
+    out = b"\x89PNG\r\n\x1a\n" + chunk(b"IHDR", struct.pack(">IIBBBBB", w, h, depth, ctype, 0, 0, int(interlace)))
+    if palette is not None:
+        out += chunk(b"PLTE", palette.astype(np.uint8).tobytes())
+    return out + chunk(b"IDAT", zlib.compress(body)) + chunk(b"IEND", b"")
+
+
+@pytest.mark.parametrize("interlace", [False, True])
+@pytest.mark.parametrize("ctype,depth", [(0, 1), (0, 2), (0, 4), (0, 16), (2, 16), (4, 16), (6, 16),
+                                         (3, 1), (3, 2), (3, 4), (3, 8), (2, 8)])
+def test_png_decoder_depths_palettes_interlace(tmp_path, ctype, depth, interlace):
+    # image::open(..).into_rgb8(): palette -> its RGB entry, sub-8-bit grey
+    # scaled to 0..255, 16-bit rounded to the nearest 8-bit value, alpha dropped
+    rng = np.random.default_rng(ctype * 100 + depth)
+    h, w = 13, 11  # odd sizes: partial Adam7 passes and partial bytes
+    channels = {0: 1, 2: 3, 3: 1, 4: 2, 6: 4}[ctype]
+    top = (1 << depth) - 1
+    palette = None
+    if ctype == 3:
+        palette = rng.integers(0, 256, (top + 1, 3))
+    samples = rng.integers(0, top + 1, (h, w, channels))
+    p = tmp_path / "t.png"
+    p.write_bytes(_png_generic(samples, ctype, depth, palette, interlace))
+    got = I.read_png(str(p))
+    if ctype == 3:
+        want = palette[samples[:, :, 0]]
+    else:
+        if depth == 16:
+            s8 = (samples * 255 + 32767) // 65535
+        else:
+            s8 = samples * 255 // top
+        want = np.repeat(s8[:, :, :1], 3, axis=2) if channels <= 2 else s8[:, :, :3]
+    np.testing.assert_array_equal(got, want.astype(np.uint8))
+    if depth <= 8:  # OpenCV's decoder (libpng) agrees where its 8-bit conversion is the same
+        cv2 = pytest.importorskip("cv2")
+        ref = cv2.imread(str(p), cv2.IMREAD_COLOR)[:, :, ::-1]
+        np.testing.assert_array_equal(got, ref)

@@ -247,6 +247,33 @@ def _models(path):
     return np.array(v, np.float32), np.array(vt, np.float32), np.array(vn, np.float32), models, mtllib
 
 
+def _mesh_of(mdl, v, vt, vn, slot):
+    """One model as a Mesh with a single material slot (tobj GPU_LOAD_OPTIONS:
+    triangulated, one index per distinct (position, texcoord, normal))."""
+    c = np.asarray(mdl["faces"], np.int64).reshape(-1, 3)  # corners: (v, vt, vn), -1 = absent
+    has_uv = len(vt) > 0 and bool((c[:, 1] >= 0).all())
+    has_n = len(vn) > 0 and bool((c[:, 2] >= 0).all())
+    key = c.copy()
+    if not has_uv:
+        key[:, 1] = -1
+    if not has_n:
+        key[:, 2] = -1
+    # single index per distinct (v, vt, vn), numbered in order of first use
+    uniq, first, inverse = np.unique(key, axis=0, return_index=True, return_inverse=True)
+    order = np.argsort(first, kind="stable")
+    rank = np.empty(len(order), np.int64)
+    rank[order] = np.arange(len(order))
+    tris = rank[inverse.reshape(-1)].reshape(-1, 3)
+    corner = uniq[order]
+    pos = v[corner[:, 0]]
+    uv = vt[corner[:, 1]] if has_uv else None
+    nrm = vn[corner[:, 2]] if has_n else None
+    return Mesh(np.ascontiguousarray(pos, np.float32), tris.astype(np.uint32),
+                normals=None if nrm is None else np.ascontiguousarray(nrm, np.float32),
+                material_slots=np.array([slot], np.uint32),
+                tex_coords=None if uv is None else np.ascontiguousarray(uv, np.float32))
+
+
 def load_obj_scene(scene, path, transform=None):
     """Adds the OBJ file's models to `scene` as objects placed by `transform`
     (4x4 row-major, default identity); returns the new object indices."""
@@ -264,28 +291,19 @@ def load_obj_scene(scene, path, transform=None):
     inv = np.linalg.inv(xf.astype(np.float64)).astype(np.float32)
     objects = []
     for mdl in models:
-        c = np.asarray(mdl["faces"], np.int64).reshape(-1, 3)  # corners: (v, vt, vn), -1 = absent
-        has_uv = len(vt) > 0 and bool((c[:, 1] >= 0).all())
-        has_n = len(vn) > 0 and bool((c[:, 2] >= 0).all())
-        key = c.copy()
-        if not has_uv:
-            key[:, 1] = -1
-        if not has_n:
-            key[:, 2] = -1
-        # single index per distinct (v, vt, vn), numbered in order of first use
-        uniq, first, inverse = np.unique(key, axis=0, return_index=True, return_inverse=True)
-        order = np.argsort(first, kind="stable")
-        rank = np.empty(len(order), np.int64)
-        rank[order] = np.arange(len(order))
-        tris = rank[inverse.reshape(-1)].reshape(-1, 3)
-        corner = uniq[order]
-        pos = v[corner[:, 0]]
-        uv = vt[corner[:, 1]] if has_uv else None
-        nrm = vn[corner[:, 2]] if has_n else None
         slot = names.index(mdl["mat"]) if mdl["mat"] in names else 0
-        mesh = Mesh(np.ascontiguousarray(pos, np.float32), tris.astype(np.uint32),
-                    normals=None if nrm is None else np.ascontiguousarray(nrm, np.float32),
-                    material_slots=np.array([slot], np.uint32),
-                    tex_coords=None if uv is None else np.ascontiguousarray(uv, np.float32))
+        mesh = _mesh_of(mdl, v, vt, vn, slot)
         objects.append(scene.add_object(Object(scene.add_mesh(mesh), list(mat_ids), xf, inv)))
     return objects
+
+
+def load_obj_meshes(path):
+    """TriangleMesh::load_obj (src/primitives/mesh.rs:19-73): the OBJ file's
+    models as meshes; each mesh's one material slot is its model's index in
+    the MTL file's material list (0 without one)."""
+    base = os.path.dirname(os.path.abspath(path))
+    v, vt, vn, models, mtllib = _models(path)
+    names = []
+    if mtllib and os.path.exists(os.path.join(base, mtllib)):
+        names = list(parse_mtl(os.path.join(base, mtllib)).keys())
+    return [_mesh_of(m, v, vt, vn, names.index(m["mat"]) if m["mat"] in names else 0) for m in models]

@@ -380,3 +380,18 @@ def test_png_decoder_depths_palettes_interlace(tmp_path, ctype, depth, interlace
         cv2 = pytest.importorskip("cv2")
         ref = cv2.imread(str(p), cv2.IMREAD_COLOR)[:, :, ::-1]
         np.testing.assert_array_equal(got, ref)
+
+
+def test_load_obj_meshes(tmp_path):
+    # TriangleMesh::load_obj: meshes only, slot = the model's MTL material index
+    (tmp_path / "scene.mtl").write_text(MTL)
+    (tmp_path / "scene.obj").write_text(OBJ)
+    meshes = I.load_obj_meshes(str(tmp_path / "scene.obj"))
+    assert [int(m.material_slots[0]) for m in meshes] == [2, 1, 4, 0]
+    assert [m.num_triangles for m in meshes] == [2, 1, 3, 1]
+    sc = SceneData()
+    objs = I.load_obj_scene(sc, str(tmp_path / "scene.obj"))
+    for m, o in zip(meshes, objs):
+        ms = sc.meshes[sc.objects[o].mesh]
+        np.testing.assert_array_equal(m.positions, ms.positions)
+        np.testing.assert_array_equal(m.indices, ms.indices)

@@ -98,20 +98,40 @@ __device__ __forceinline__ void deposit(const EngineDev& E, uint32_t job, uint32
     count_done(E, job);
 }
 
-// Free slots -> samples of the active jobs, oldest first.
+// Free slots -> samples of the active jobs.  Each job with samples left is
+// first offered an equal share of the free slots (so a small job finishes in
+// the tick it arrives instead of waiting behind a large one), then what the
+// shares leave goes to the jobs oldest first; every free slot is used as
+// before, only the split changes.  Images do not depend on the split: every
+// sample is keyed by (job seed, pixel, sample).
 __global__ void k_plan(EngineDev E, int q) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     const uint32_t n_cont = E.cnt[q];
     uint32_t used = 0, nseg = 0;
     const uint32_t na = *E.n_active;
-    for (uint32_t a = 0; a < na && n_cont + used < E.capacity; ++a) {
+    const uint32_t free_paths = E.capacity - n_cont;
+    uint32_t waiting = 0;
+    for (uint32_t a = 0; a < na; ++a) {
+        const JobDev& J = E.jobs[E.active[a]];
+        if (J.total_samples > J.next_sample) waiting++;
+    }
+    const uint32_t share = waiting ? free_paths / waiting : 0;
+    uint32_t left = free_paths;
+    for (uint32_t a = 0; a < na; ++a) {  // the equal shares
+        const JobDev& J = E.jobs[E.active[a]];
+        const unsigned long long rem = J.total_samples - J.next_sample;
+        left -= uint32_t(min(rem, (unsigned long long)(share / J.roles))) * J.roles;
+    }
+    for (uint32_t a = 0; a < na; ++a) {  // shares plus the remainder, oldest first
         const uint32_t j = E.active[a];
         JobDev& J = E.jobs[j];
         const unsigned long long rem = J.total_samples - J.next_sample;
         if (rem == 0) continue;
-        const uint32_t free_paths = E.capacity - n_cont - used;
-        const unsigned long long take = min(rem, (unsigned long long)(free_paths / J.roles));
-        if (take == 0) break;
+        const unsigned long long fair = min(rem, (unsigned long long)(share / J.roles));
+        const unsigned long long extra = min(rem - fair, (unsigned long long)(left / J.roles));
+        left -= uint32_t(extra) * J.roles;
+        const unsigned long long take = fair + extra;
+        if (take == 0) continue;
         E.plan[nseg] = Segment{j, n_cont + used, uint32_t(take), J.roles, J.next_sample};
         J.next_sample += take;
         used += uint32_t(take) * J.roles;

@@ -295,13 +295,24 @@ struct ServerImpl {
         std::vector<BdJob> jobs;
         std::vector<BdSegment> segs;
         std::vector<SJob*> members;
+        // Each waiting job is offered an equal share of the batch, then what
+        // the shares leave goes oldest first (as the PT tick plan does).
         const uint32_t cap = bdpt_batch_capacity(bdpt);
+        uint32_t waiting = 0;
+        for (SJob* j : active_bd) waiting += j->bd_issued ? 0u : 1u;
+        const uint32_t share = waiting ? cap / waiting : 0;
+        uint32_t left = cap;
+        for (SJob* j : active_bd)
+            if (!j->bd_issued) left -= uint32_t(std::min<uint64_t>(j->samples - j->bd_next, share));
         uint32_t used = 0;
         for (SJob* j : active_bd) {
             if (j->bd_issued) continue;
-            if (used >= cap) break;
             const uint64_t rem = j->samples - j->bd_next;
-            const uint32_t take = uint32_t(std::min<uint64_t>(rem, cap - used));
+            const uint64_t fair = std::min<uint64_t>(rem, share);
+            const uint64_t extra = std::min<uint64_t>(rem - fair, left);
+            left -= uint32_t(extra);
+            const uint32_t take = uint32_t(fair + extra);
+            if (take == 0) continue;
             const CameraDev cam = make_camera(j->cam);
             segs.push_back(BdSegment{uint32_t(jobs.size()), used, take, 0, j->bd_next});
             jobs.push_back(make_bdpt_job(j->scene, cam, j->cfg, j->w, j->h, j->films));

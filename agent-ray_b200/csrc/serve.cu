@@ -3,12 +3,14 @@
 //
 // One worker thread owns two internal contexts (streams) on the device:
 //   * the PT stream runs the streaming path engine (PT and GDPT jobs); every
-//     admitted job's samples flow into the same path pool, oldest job first;
-//   * the BDPT stream runs sample batches that mix every active BDPT job.
+//     admitted job's samples flow into the same path pool, free slots split
+//     in equal shares among the jobs with samples left, the rest oldest first;
+//   * the BDPT stream runs sample batches that mix every active BDPT job,
+//     split the same way.
 // Admission is FIFO under an HBM budget for job films; completion is detected
 // from pinned snapshots of the per-job done counters (PT) or batch events
 // (BDPT), then the film is converted (GDPT: Poisson-reconstructed) and copied
-// to the caller's host buffer before the job reports DONE.
+// to the caller's host or device buffer before the job reports DONE.
 #include <algorithm>
 #include <atomic>
 #include <chrono>

@@ -186,3 +186,26 @@ def test_oracle_dielectric_scene_is_finite_and_transmits():
     plain, _ = S.cornell_box(1)
     other = O.OracleScene(plain).render(cam, integrator_cfg(A.INTEGRATOR_PT, spp=32, max_depth=8, seed=3), 24, 24)
     assert np.abs(img - other).mean() > 1e-3
+
+
+def test_header_is_plain_c_with_ctypes_layouts(tmp_path):
+    # The boundary header compiles as strict C99 (what cgo / bindgen / a C
+    # caller sees), and its struct sizes equal the Python mirror's.
+    import subprocess
+    from agentray import _abi as A
+    structs = {"ar_mesh_desc": A.MeshDesc, "ar_object_desc": A.ObjectDesc, "ar_material_desc": A.MaterialDesc,
+               "ar_texture_desc": A.TextureDesc, "ar_light_desc": A.LightDesc, "ar_scene_desc": A.SceneDesc,
+               "ar_camera_desc": A.CameraDesc, "ar_integrator_cfg": A.IntegratorCfg, "ar_ray_batch": A.RayBatch,
+               "ar_hit": A.Hit, "ar_accel_opts": A.AccelOpts, "ar_scene_stats": A.SceneStats,
+               "ar_tuning": A.Tuning, "ar_tune_opts": A.TuneOpts, "ar_tune_result": A.TuneResult,
+               "ar_server_opts": A.ServerOpts, "ar_job_info": A.JobInfo, "ar_server_stats": A.ServerStats,
+               "ar_render_stats": A.RenderStats}
+    src = tmp_path / "h.c"
+    src.write_text('#include <stdio.h>\n#include "agentray.h"\nint main(void) {\n' +
+                   "".join(f'    printf("%zu\\n", sizeof({n}));\n' for n in structs) + "    return 0;\n}\n")
+    exe = tmp_path / "h"
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic",
+                    "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    sizes = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    import ctypes
+    assert sizes == [ctypes.sizeof(t) for t in structs.values()], dict(zip(structs, sizes))

@@ -114,6 +114,8 @@ def test_png_writer_round_trip(tmp_path):
 
 
 def test_ns_to_roughness():
+    # the crate's design notes: Ns=0 -> alpha=1 (rough), Ns=1000 -> alpha~0.044
+    assert I.ns_to_roughness(1000.0) == pytest.approx(0.044, abs=1e-3)
     assert I.ns_to_roughness(0.0) == 1.0
     assert I.ns_to_roughness(1e9) == pytest.approx(1e-3)  # clamped at the low end
     assert I.ns_to_roughness(98.0) == pytest.approx(np.sqrt(2.0 / 100.0), rel=1e-6)
@@ -395,3 +397,12 @@ def test_load_obj_meshes(tmp_path):
         ms = sc.meshes[sc.objects[o].mesh]
         np.testing.assert_array_equal(m.positions, ms.positions)
         np.testing.assert_array_equal(m.indices, ms.indices)
+
+
+def test_mtl_defaults(tmp_path):
+    # an MTL material with no statements: Kd 0.5 grey, Ks 0, Ns 0, d 1, Ni 1.5
+    # -> a grey Lambertian (the crate's defaults)
+    (tmp_path / "e.mtl").write_text("newmtl empty\n")
+    sc = SceneData()
+    m = I.convert_material(I.parse_mtl(str(tmp_path / "e.mtl"))["empty"], str(tmp_path), sc)
+    assert m.kind == A.MATERIAL_LAMBERTIAN and m.albedo == (0.5, 0.5, 0.5) and m.albedo_texture == -1

@@ -50,6 +50,23 @@ int guarded(F&& f) {
     }
 }
 
+// Fails with AR_ERR_INVALID_ARGUMENT unless `p` is device (or managed) memory
+// that `device` can address: a host pointer or another GPU's buffer handed to
+// a kernel would fault the GPU instead of returning an error.  Allocates
+// nothing; safe during stream capture.
+inline void require_device_ptr(const void* p, int device, const char* what) {
+    cudaPointerAttributes a{};
+    const cudaError_t e = cudaPointerGetAttributes(&a, p);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        throw ArError{AR_ERR_INVALID_ARGUMENT, std::string(what) + ": not a CUDA pointer"};
+    }
+    const bool dev = a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    if (!dev || (a.type == cudaMemoryTypeDevice && a.device != device))
+        throw ArError{AR_ERR_INVALID_ARGUMENT,
+                      std::string(what) + ": not device memory of device " + std::to_string(device)};
+}
+
 // Device buffer owned by a scene or context.
 struct DevBuf {
     void* ptr = nullptr;

@@ -234,9 +234,16 @@ int ar_poisson_reconstruct(ar_context* ctx, const ar_integrator_cfg* cfg, uint32
     return guarded([&] {
         AR_REQUIRE(ctx && cfg && primal && grad_x && grad_y && out, AR_ERR_INVALID_ARGUMENT, "null argument");
         AR_REQUIRE(width > 0 && height > 0, AR_ERR_INVALID_ARGUMENT, "empty image");
+        // the solver kernels index interleaved RGB planes with 32-bit offsets
+        AR_REQUIRE(uint64_t(width) * height * 3 <= UINT32_MAX, AR_ERR_INVALID_ARGUMENT,
+                   "image too large for the Poisson solver (W*H*3 must fit in 32 bits)");
         AR_CUDA(cudaSetDevice(ctx->device));
         const size_t count = size_t(width) * height * 3;
         if (on_device) {
+            require_device_ptr(primal, ctx->device, "primal");
+            require_device_ptr(grad_x, ctx->device, "grad_x");
+            require_device_ptr(grad_y, ctx->device, "grad_y");
+            require_device_ptr(out, ctx->device, "out");
             poisson_reconstruct(ctx, *cfg, width, height, primal, grad_x, grad_y, out, rel_residual);
             return;
         }

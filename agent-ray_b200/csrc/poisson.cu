@@ -236,14 +236,7 @@ void poisson_reconstruct(ar_context* ctx, const ar_integrator_cfg& cfg, uint32_t
     if (cfg.poisson_solver == AR_POISSON_SOR) {
         ctx->solver.ensure(2 * 3 * n * sizeof(float));
         float* rhs = ctx->solver.buf.as<float>();
-        float* img = rhs + 3 * n;
-        k_rhs<<<grid, 256, 0, st>>>(w, h, primal, gx, gy, cfg.alpha,
-                                     (cfg.gdpt_flags & AR_GDPT_CONSISTENT_DIVERGENCE) != 0, rhs, img);
-        for (uint32_t it = 0; it < cfg.poisson_iterations; ++it)
-            for (uint32_t parity = 0; parity < 2; ++parity)
-                k_sor_half<<<grid, 256, 0, st>>>(w, h, parity, rhs, img, cfg.alpha, cfg.sor_omega);
-        k_clamp<<<grid, 256, 0, st>>>(3 * n, img, out);
-        AR_CUDA(cudaGetLastError());
+        poisson_sor_with_scratch(st, ctx->num_sms, cfg, w, h, primal, gx, gy, rhs, rhs + 3 * n, out);
         if (rel_residual) *rel_residual = -1.0;
         return;
     }

@@ -65,6 +65,8 @@ extern "C" int ar_poisson_sor_static(const ar_integrator_cfg* cfg, uint32_t widt
                                      void* cuda_stream) {
     return guarded([&] {
         AR_REQUIRE(cfg && primal && grad_x && grad_y && out, AR_ERR_INVALID_ARGUMENT, "null argument");
+        AR_REQUIRE(cfg->poisson_solver == AR_POISSON_SOR, AR_ERR_UNSUPPORTED,
+                   "ar_poisson_sor_static solves with red-black SOR only (cfg->poisson_solver must be AR_POISSON_SOR)");
         AR_REQUIRE(width > 0 && height > 0, AR_ERR_INVALID_ARGUMENT, "empty image");
         AR_REQUIRE(uint64_t(width) * height <= kStaticSorMaxPixels, AR_ERR_INVALID_ARGUMENT,
                    "image of " + std::to_string(uint64_t(width) * height) + " pixels exceeds the static scratch (" +
@@ -72,6 +74,10 @@ extern "C" int ar_poisson_sor_static(const ar_integrator_cfg* cfg, uint32_t widt
         int device = 0;
         AR_CUDA(cudaGetDevice(&device));
         AR_REQUIRE(device >= 0 && device < kMaxDevices, AR_ERR_UNSUPPORTED, "device ordinal too large");
+        require_device_ptr(primal, device, "primal");
+        require_device_ptr(grad_x, device, "grad_x");
+        require_device_ptr(grad_y, device, "grad_y");
+        require_device_ptr(out, device, "out");
         float* scratch = scratch_for(device);
         float* rhs = scratch;
         float* img = scratch + 3 * size_t(kStaticSorMaxPixels);

@@ -354,8 +354,10 @@ int ar_poisson_reconstruct(ar_context* ctx, const ar_integrator_cfg* cfg, uint32
  * that cannot allocate device memory while they run: a frame loop or a plugin
  * whose host owns the device memory pool, or code between CUDA-graph captures
  * where cudaMalloc would synchronise.  Same result as ar_poisson_reconstruct
- * with AR_POISSON_SOR, but: all pointers are device pointers on the current
- * device; work is queued on `cuda_stream` (NULL: the legacy default stream)
+ * with AR_POISSON_SOR (cfg->poisson_solver must be AR_POISSON_SOR, else
+ * AR_ERR_UNSUPPORTED), but: all pointers are device pointers on the current
+ * device (anything else fails with AR_ERR_INVALID_ARGUMENT before any launch);
+ * work is queued on `cuda_stream` (NULL: the legacy default stream)
  * without synchronising; no context is needed and nothing is allocated.  The
  * solver's scratch is a static device array of 6 MiB that every GPU loading the
  * library keeps until exit, which limits images to AR_STATIC_SOR_MAX_PIXELS

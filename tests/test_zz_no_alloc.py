@@ -63,3 +63,19 @@ def test_static_sor_rejects_images_beyond_its_scratch(ctx):
                                               buf.data_ptr(), None)
     assert rc == A.AR_ERR_INVALID_ARGUMENT
     assert b"exceeds the static scratch" in agentray.lib().ar_last_error()
+
+
+def test_static_sor_rejects_other_solvers_and_host_pointers(ctx):
+    # It solves with SOR only: a CG request is refused, not silently served by
+    # SOR.  Host arrays are refused before any kernel could touch them.
+    import torch
+    buf = torch.zeros(16 * 16 * 3, dtype=torch.float32, device="cuda")
+    p = buf.data_ptr()
+    cg = integrator_cfg(A.INTEGRATOR_GDPT, poisson_solver=A.POISSON_CG)
+    rc = agentray.lib().ar_poisson_sor_static(C.byref(cg), 16, 16, p, p, p, p, None)
+    assert rc == A.AR_ERR_UNSUPPORTED
+    host = np.zeros(16 * 16 * 3, np.float32)
+    sor = integrator_cfg(A.INTEGRATOR_GDPT, poisson_solver=A.POISSON_SOR)
+    rc = agentray.lib().ar_poisson_sor_static(C.byref(sor), 16, 16, p, p, p, host.ctypes.data, None)
+    assert rc == A.AR_ERR_INVALID_ARGUMENT
+    assert b"not device memory" in agentray.lib().ar_last_error()

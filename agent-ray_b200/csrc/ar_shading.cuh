@@ -1,7 +1,9 @@
 // Device shading layer: shading points, BSDFs, lights and the camera.
 // Mirrors the reference operation order; translation units that include this
 // are compiled with -fmad=false so no multiply is fused into an add (the
-// reference Rust/glam code rounds each operation separately).
+// reference Rust/glam code rounds each operation separately).  Sines and
+// cosines of sampling angles come from ar_trig.h, which the CPU oracle uses
+// too, so both sides draw bit-identical directions.
 //   Scene::intersect shading     src/scene.rs:142-162, :55-87
 //   Onb                          src/geometry.rs:218-244
 //   Lambertian                   src/surfaces/lambertian.rs:35-64
@@ -15,6 +17,7 @@
 #pragma once
 #include "ar_device.cuh"
 #include "ar_render.hpp"
+#include "ar_trig.h"
 
 namespace ar {
 
@@ -92,7 +95,9 @@ __device__ __forceinline__ bool same_hemi(f3 a, f3 b) { return a.z * b.z > 0.f; 
 __device__ __forceinline__ f3 cosine_hemisphere(float ux, float uy) {
     float r = sqrtf(ux);
     float phi = (2.0f * kPi) * uy;
-    float x = r * cosf(phi), y = r * sinf(phi);
+    float sp, cp;
+    ar_trig::sincos(phi, &sp, &cp);
+    float x = r * cp, y = r * sp;
     float z = sqrtf(fmaxf((1.0f - x * x) - y * y, 0.0f));
     return mk(x, y, z);
 }
@@ -286,7 +291,9 @@ __device__ __forceinline__ bool bsdf_sample(const MatView& m, f3 wo, float u_sel
     float c2 = (1.0f - ux) / ((a2 - 1.0f) * ux + 1.0f);
     float ch = sqrtf(fmaxf(c2, 0.f)), sh = sqrtf(fmaxf(1.0f - c2, 0.f));
     float phi = (2.0f * kPi) * uy;
-    f3 h = mk(sh * cosf(phi), sh * sinf(phi), ch);
+    float sp, cp;
+    ar_trig::sincos(phi, &sp, &cp);
+    f3 h = mk(sh * cp, sh * sp, ch);
     if (h.z * wo.z < 0.f) h = -h;
     if (m.kind == AR_MATERIAL_DIELECTRIC && !(u_sel < fresnel_dielectric(fabsf(dot(wo, h)), m.eta))) {
         const float eta = wo.z > 0.f ? 1.0f / m.eta : m.eta;

@@ -146,7 +146,9 @@ __device__ __forceinline__ f3 uniform_sphere(float ux, float uy) {
     const float ct = 1.0f - 2.0f * ux;
     const float st = sqrtf(fmaxf(1.0f - ct * ct, 0.0f));
     const float phi = (2.0f * kPi) * uy;
-    return mk(st * cosf(phi), st * sinf(phi), ct);
+    float sp, cp;
+    ar_trig::sincos(phi, &sp, &cp);
+    return mk(st * cp, st * sp, ct);
 }
 
 __device__ __forceinline__ bool mis_delta(const Vtx& v) { return v.type == kTypeSurface && v.delta; }

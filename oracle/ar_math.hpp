@@ -12,7 +12,20 @@
 #include <cfloat>
 #include <limits>
 
+#include "../agent-ray_b200/csrc/ar_trig.h"
+
 namespace oracle {
+
+// Sine and cosine of a sampling angle.  The FP32 oracle takes them from
+// ar_trig.h, the single-precision routine the kernels use too, so the GPU and
+// the oracle draw bit-identical directions (libm's sinf/cosf, which the Rust
+// reference's f32::sin/cos reach, differ from it by at most about 1e-7 in
+// absolute terms); the FP64 oracle uses the double-precision library.
+inline void sin_cos(float phi, float& s, float& c) { ar_trig::sincos(phi, &s, &c); }
+inline void sin_cos(double phi, double& s, double& c) {
+    s = std::sin(phi);
+    c = std::cos(phi);
+}
 
 template <class T> struct V2 { T x, y; };
 

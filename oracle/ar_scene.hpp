@@ -48,8 +48,10 @@ template <class T>
 inline V3<T> cosine_hemisphere_sample(V2<T> u) {
     T r = std::sqrt(u.x);
     T phi = (T(2) * pi<T>()) * u.y;
-    T x = r * std::cos(phi);
-    T y = r * std::sin(phi);
+    T sp, cp;
+    sin_cos(phi, sp, cp);
+    T x = r * cp;
+    T y = r * sp;
     T z = std::sqrt(rmax((T(1) - x * x) - y * y, T(0)));
     return {x, y, z};
 }
@@ -93,7 +95,9 @@ inline V3<T> ggx_sample_wh(T alpha, V3<T> wo, V2<T> u) {
     T ch = std::sqrt(rmax(c2, T(0)));
     T sh = std::sqrt(rmax(T(1) - c2, T(0)));
     T phi = (T(2) * pi<T>()) * u.y;
-    V3<T> h(sh * std::cos(phi), sh * std::sin(phi), ch);
+    T sp, cp;
+    sin_cos(phi, sp, cp);
+    V3<T> h(sh * cp, sh * sp, ch);
     if (h.z * wo.z < T(0)) h = -h;
     return h;
 }
@@ -319,7 +323,9 @@ inline V3<T> uniform_sphere_sample(V2<T> u) {
     T ct = T(1) - T(2) * u.x;
     T st = std::sqrt(rmax(T(1) - ct * ct, T(0)));
     T phi = (T(2) * pi<T>()) * u.y;
-    return {st * std::cos(phi), st * std::sin(phi), ct};
+    T sp, cp;
+    sin_cos(phi, sp, cp);
+    return {st * cp, st * sp, ct};
 }
 
 template <class T>

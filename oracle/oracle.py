@@ -42,6 +42,7 @@ def lib():
         lb.oracle_poisson_exact_f64.argtypes = [u32, u32, vp, vp, vp, C.c_double, C.c_double, u32, vp, vp]
         lb.oracle_counter_u01.argtypes = [u64, u32, u32, u32, u32, vp]
         lb.oracle_xoshiro_f32.argtypes = [u32, u32, u32, vp]
+        lb.oracle_sincos_f32.argtypes = [vp, u64, vp, vp]
         lb.oracle_blas_stats.argtypes = [vp, u32, vp]
         lb.oracle_film_to_rgb8.argtypes = [vp, u32, u32, u32, C.c_float, C.c_float, C.c_float, vp]
         lb.oracle_texture_sample.argtypes = [vp, u32, u32, vp, u32, vp]
@@ -155,6 +156,15 @@ def xoshiro_f32(px, py, n):
     out = np.empty(n, np.float32)
     lib().oracle_xoshiro_f32(px, py, n, _p(out))
     return out
+
+
+def sincos_f32(x):
+    """(sin, cos) of float32 angles as the FP32 oracle (and the kernels) compute them."""
+    x = np.ascontiguousarray(x, np.float32)
+    s = np.empty_like(x)
+    c = np.empty_like(x)
+    lib().oracle_sincos_f32(_p(x), x.size, _p(s), _p(c))
+    return s, c
 
 
 def film_to_rgb8(hdr, tone_mapper=0, white_point=1.0, gamma=2.2, scale=1.0):

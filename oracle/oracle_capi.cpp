@@ -211,6 +211,12 @@ int oracle_xoshiro_f32(uint32_t px, uint32_t py, uint32_t n, float* out) {
     return 0;
 }
 
+// sin and cos of n FP32 angles through the routine the FP32 oracle samples with.
+int oracle_sincos_f32(const float* x, uint64_t n, float* s, float* c) {
+    for (uint64_t i = 0; i < n; ++i) sin_cos(x[i], s[i], c[i]);
+    return 0;
+}
+
 // Structure of the restated reference BVH: node count, leaf count, max depth.
 int oracle_blas_stats(void* sp, uint32_t mesh, uint64_t* out3) {
     auto* s = static_cast<OracleScene*>(sp);

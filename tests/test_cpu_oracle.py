@@ -53,6 +53,22 @@ def test_xoshiro_stream_matches_python_restatement():
     np.testing.assert_array_equal(O.xoshiro_f32(3, 5, 8), np.array(vals, np.float32))
 
 
+def test_sampling_sincos_accuracy():
+    # ar_trig.h (shared by the FP32 oracle and the kernels): every sampling
+    # angle 2*pi*u, u in [0, 1), within 1.5e-7 of float64 sin/cos; exact at
+    # the quadrant points; |s|, |c| <= 1.
+    rng = np.random.default_rng(5)
+    u = np.concatenate([rng.uniform(0, 1, 2_000_000), np.arange(1 << 16) / (1 << 16)]).astype(np.float32)
+    x = (np.float32(2 * math.pi) * u).astype(np.float32)
+    s, c = O.sincos_f32(x)
+    xd = x.astype(np.float64)
+    assert np.abs(s - np.sin(xd)).max() < 1.5e-7
+    assert np.abs(c - np.cos(xd)).max() < 1.5e-7
+    assert np.abs(s).max() <= 1.0 and np.abs(c).max() <= 1.0
+    s0, c0 = O.sincos_f32(np.zeros(1, np.float32))
+    assert s0[0] == 0.0 and c0[0] == 1.0
+
+
 def test_counter_sampler_range_and_independence():
     u = O.counter_u01(7, 12345, 3, 0, 100000)
     assert u.min() >= 0.0 and u.max() < 1.0

@@ -145,7 +145,8 @@ class ServerStats(C.Structure):
     _fields_ = [("jobs_submitted", C.c_uint64), ("jobs_done", C.c_uint64), ("jobs_rejected", C.c_uint64),
                 ("jobs_cancelled", C.c_uint64), ("jobs_failed", C.c_uint64), ("path_samples_done", C.c_uint64),
                 ("pt_ticks", C.c_uint64), ("bdpt_batches", C.c_uint64), ("film_bytes_in_use", C.c_uint64),
-                ("film_bytes_peak", C.c_uint64)]
+                ("film_bytes_peak", C.c_uint64), ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64),
+                ("kernel_launches", C.c_uint64)]
 
 
 class RenderStats(C.Structure):

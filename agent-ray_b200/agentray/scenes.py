@@ -112,8 +112,8 @@ def cornell_box(seed=1, light_radiance=15.0, point_light=False, glass=False, tex
     """Config-1 Cornell box: 5 walls (10 tris) + 2 rotated boxes (24 tris) and a
     0.25 x 0.25 quad light of radiance 15 just below the ceiling.  textured=True
     gives the floor and back wall checker ImageTextures.  glass=True
-    makes the tall box a rough dielectric (eta 1.5, alpha 0.2) and adds a
-    dielectric icosphere (eta 1.33, alpha 0.05)."""
+    makes the tall box a rough dielectric (eta 1.5, alpha 0.2), lifted 2 mm
+    off the floor, and adds a dielectric icosphere (eta 1.33, alpha 0.05)."""
     rng = np.random.default_rng(seed)
     sc = SceneData(A.LIGHT_DIST_POWER)
     walls = [((0, 0, 0), (0, 0, 1), (1, 0, 0)),   # floor
@@ -139,6 +139,11 @@ def cornell_box(seed=1, light_radiance=15.0, point_light=False, glass=False, tex
         mat = sc.add_material(Material(A.MATERIAL_LAMBERTIAN, albedo=tuple(rng.uniform(0.2, 0.8, 3))))
         if glass and k == 0:
             mat = sc.add_material(Material(A.MATERIAL_DIELECTRIC, roughness=0.2, eta=1.5))
+            # lifted 2 mm off the floor: a glass box standing on it would put
+            # its bottom face in the floor's plane, and a ray leaving the box
+            # downward would hit both at the same t (a tie that any two
+            # traversal orders may break differently)
+            ty += 0.002
         xf, inv = trs((tx, ty, tz), rot_y(deg), (sx, sy, sz))
         sc.add_object(Object(cube, [mat], xf, inv))
     if glass:

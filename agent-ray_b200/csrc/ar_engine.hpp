@@ -23,6 +23,8 @@
 namespace ar {
 
 constexpr uint32_t kMaxActiveJobs = 1024;
+// Kernels in one tick: plan, generate, extend, shade, shadow.
+constexpr uint32_t kEngineTickKernels = 5;
 
 // Device job-table entry.
 struct alignas(16) JobDev {
@@ -50,8 +52,9 @@ void engine_add_job(PathEngine* e, uint32_t slot, const JobDev& job);
 // Removes a finished job from the active list.
 void engine_remove_job(PathEngine* e, uint32_t slot);
 // Batched form of the two calls above: one staged upload for many changes.
-void engine_update(PathEngine* e, const std::vector<std::pair<uint32_t, JobDev>>& adds,
-                   const std::vector<uint32_t>& removes);
+// Returns the bytes copied host -> device.
+size_t engine_update(PathEngine* e, const std::vector<std::pair<uint32_t, JobDev>>& adds,
+                     const std::vector<uint32_t>& removes);
 // Enqueues one tick (graph replay) on the context stream.
 void engine_tick(PathEngine* e);
 // Enqueues an async copy of every job's done_paths into pinned host memory;

@@ -30,7 +30,8 @@ void render_bdpt_film(ar_context* ctx, const ar_scene* sc, const CameraDev& cam,
 
 // Screened-Poisson reconstruction on the device.  Inputs are interleaved RGB
 // f32 films (W*H*3); `out` receives the clamped reconstruction.
-void poisson_reconstruct(ar_context* ctx, const ar_integrator_cfg& cfg, uint32_t w, uint32_t h, const float* primal,
+// Returns the number of kernels launched.
+uint64_t poisson_reconstruct(ar_context* ctx, const ar_integrator_cfg& cfg, uint32_t w, uint32_t h, const float* primal,
                          const float* gx, const float* gy, float* out, double* rel_residual);
 
 // Converts an f64 film to f32 (or copies an f32 film) into `out`.

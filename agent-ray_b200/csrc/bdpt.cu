@@ -44,9 +44,9 @@ constexpr uint32_t kBdShadowCursor = 127, kBdExtendCursor = 128, kBdBins = 256, 
 struct BdParams {
     const BdJob* jobs;
     const BdSegment* seg;
-    uint32_t nseg;
-    uint32_t nsamples;  // samples in this batch
-    uint32_t maxv;      // vertex capacity per subpath
+    const uint32_t* dyn;  // device: [0] samples in this batch, [1] segments (set per batch)
+    uint32_t cap;         // batch capacity: the stride of the per-sample arrays
+    uint32_t maxv;        // vertex capacity per subpath
     uint32_t* sjob;     // job of each batch sample
     unsigned long long* sindex;  // global sample index of each batch sample
     float4* va;  // p.xyz, pdf_fwd
@@ -57,7 +57,7 @@ struct BdParams {
     float4* svb; // order, so the connection kernel's warps read them coalesced
     float4* svc;
     float2* svuv;
-    uint8_t* nv; // [sub * nsamples + si]
+    uint8_t* nv; // [sub * cap + si]
     float4* thr; // per subpath q = 2 si + sub: thr.xyz, previous directional pdf
     uint32_t* dim;
     float4* ray_o[2];
@@ -77,7 +77,7 @@ struct BdParams {
 };
 
 __device__ __forceinline__ size_t vidx(const BdParams& P, uint32_t sub, uint32_t k, uint32_t si) {
-    return (size_t(sub) * P.maxv + k) * P.nsamples + si;
+    return (size_t(sub) * P.maxv + k) * P.cap + si;
 }
 
 struct Vtx {
@@ -299,13 +299,14 @@ __device__ __forceinline__ void push_shadow(const BdParams& P, uint32_t job, f3 
 }
 
 __global__ void __launch_bounds__(256) k_bd_generate(BdParams P) {
-    for (uint32_t base = blockIdx.x * blockDim.x; base < 2 * P.nsamples; base += gridDim.x * blockDim.x) {
+    const uint32_t ns = P.dyn[0], nseg = P.dyn[1];
+    for (uint32_t base = blockIdx.x * blockDim.x; base < 2 * ns; base += gridDim.x * blockDim.x) {
         const uint32_t q = base + threadIdx.x;
-        bool live = q < 2 * P.nsamples;
+        bool live = q < 2 * ns;
         const uint32_t si = q >> 1, sub = q & 1u;
         Ray r{};
         if (live) {
-            uint32_t lo = 0, hi = P.nseg;
+            uint32_t lo = 0, hi = nseg;
             while (hi - lo > 1) {
                 const uint32_t mid = (lo + hi) >> 1;
                 if (P.seg[mid].offset <= si) lo = mid; else hi = mid;
@@ -357,17 +358,17 @@ __global__ void __launch_bounds__(256) k_bd_generate(BdParams P) {
                     r = Ray{o, normalize(dir), 1e-4f, FLT_MAX};
                     const float pp = pdf_pos * sel;
                     store_vtx(P, 1, 0, si, o, nl, L.inten / pp, pp, kTypeLight, L.kind == AR_LIGHT_POINT, li);
-                    P.nv[P.nsamples + si] = 1;
+                    P.nv[P.cap + si] = 1;
                     f3 thr = L.inten / (pp * pdf_dir);
                     thr = thr * fabsf(dot(nl, r.d));
                     P.thr[q] = make_float4(thr.x, thr.y, thr.z, pdf_dir);
                     P.dim[q] = d;
                 } else {
-                    P.nv[P.nsamples + si] = 0;
+                    P.nv[P.cap + si] = 0;
                     live = false;
                 }
             } else {
-                P.nv[P.nsamples + si] = 0;
+                P.nv[P.cap + si] = 0;
                 live = false;
             }
             if (J.max_depth == 0) live = false;
@@ -419,14 +420,14 @@ __global__ void __launch_bounds__(256, 4) k_bd_vertex(BdParams P, uint32_t depth
                 const MatView m = load_mat_at(J.sc, s.mat, s.tu, s.tv);
                 const float4 t4 = P.thr[q];
                 f3 thr = mk(t4.x, t4.y, t4.z);
-                const uint32_t k = P.nv[sub * P.nsamples + si];  // index of the new vertex
+                const uint32_t k = P.nv[sub * P.cap + si];  // index of the new vertex
                 const size_t pi = vidx(P, sub, k - 1, si);
                 const float4 pa = P.va[pi], pb = P.vb[pi];
                 const f3 prev_p = mk(pa.x, pa.y, pa.z), prev_n = mk(pb.x, pb.y, pb.z);
                 const float pdf_fwd = pdf_sa_to_area(t4.w, prev_p, s.p, s.n);
                 store_vtx(P, sub, k, si, s.p, s.n, thr, pdf_fwd, kTypeSurface, false, s.mat,
                           J.sc.materials[s.mat].tex >= 0, s.tu, s.tv);
-                P.nv[sub * P.nsamples + si] = uint8_t(k + 1);
+                P.nv[sub * P.cap + si] = uint8_t(k + 1);
                 const unsigned long long g = P.sindex[si];
                 const uint32_t npix = J.width * J.height;
                 const uint64_t key = counter_key(J.seed, uint32_t(g % npix), uint32_t(g / npix));
@@ -616,16 +617,17 @@ __device__ void connect_s1(const BdParams& P, const BdJob& J, uint32_t job, uint
 // Counting sort of the batch samples by their subpath lengths (S, T), so the
 // warps of the connection kernel run strategy loops of equal trip counts.
 __device__ __forceinline__ uint32_t bd_sort_key(const BdParams& P, uint32_t si) {
-    const uint32_t S = P.nv[si], T = P.nv[P.nsamples + si];
+    const uint32_t S = P.nv[si], T = P.nv[P.cap + si];
     return min(S, 15u) * 16u + min(T, 15u);
 }
 
 __global__ void __launch_bounds__(256) k_bd_hist(BdParams P) {
     __shared__ uint32_t h[kBdBins];
+    const uint32_t ns = P.dyn[0];
     h[threadIdx.x] = 0;
     __syncthreads();
-    const uint32_t si = blockIdx.x * 256 + threadIdx.x;
-    if (si < P.nsamples) atomicAdd(&h[bd_sort_key(P, si)], 1u);
+    for (uint32_t si = blockIdx.x * 256 + threadIdx.x; si < ns; si += gridDim.x * 256)
+        atomicAdd(&h[bd_sort_key(P, si)], 1u);
     __syncthreads();
     if (h[threadIdx.x]) atomicAdd(&P.counts[kBdHist + threadIdx.x], h[threadIdx.x]);
 }
@@ -646,31 +648,38 @@ __global__ void __launch_bounds__(256) k_bd_scan(BdParams P) {
     P.counts[kBdOffs + threadIdx.x] = h[threadIdx.x];
 }
 
+// Chunks of 256 samples, one chunk per block at a time (the loop trip count is
+// the same for every thread of a block, so the barriers are uniform).
 __global__ void __launch_bounds__(256) k_bd_scatter(BdParams P) {
     __shared__ uint32_t h[kBdBins], base[kBdBins];
-    h[threadIdx.x] = 0;
-    __syncthreads();
-    const uint32_t si = blockIdx.x * 256 + threadIdx.x;
-    const bool live = si < P.nsamples;
-    uint32_t key = 0, rank = 0;
-    if (live) {
-        key = bd_sort_key(P, si);
-        rank = atomicAdd(&h[key], 1u);
+    const uint32_t ns = P.dyn[0];
+    for (uint32_t chunk = blockIdx.x * 256; chunk < ns; chunk += gridDim.x * 256) {
+        h[threadIdx.x] = 0;
+        __syncthreads();
+        const uint32_t si = chunk + threadIdx.x;
+        const bool live = si < ns;
+        uint32_t key = 0, rank = 0;
+        if (live) {
+            key = bd_sort_key(P, si);
+            rank = atomicAdd(&h[key], 1u);
+        }
+        __syncthreads();
+        if (h[threadIdx.x]) base[threadIdx.x] = atomicAdd(&P.counts[kBdOffs + threadIdx.x], h[threadIdx.x]);
+        __syncthreads();
+        if (live) P.order[base[key] + rank] = si;
+        __syncthreads();
     }
-    __syncthreads();
-    if (h[threadIdx.x]) base[threadIdx.x] = atomicAdd(&P.counts[kBdOffs + threadIdx.x], h[threadIdx.x]);
-    __syncthreads();
-    if (live) P.order[base[key] + rank] = si;
 }
 
 // Copies every sample's vertices to its sorted position oi (reads scattered,
 // writes coalesced), so k_bd_connect, whose thread oi handles sample
 // order[oi], reads vertex k of 32 consecutive samples as one contiguous block.
 __global__ void __launch_bounds__(256) k_bd_permute(BdParams P) {
-    for (uint32_t oi = blockIdx.x * blockDim.x + threadIdx.x; oi < P.nsamples; oi += gridDim.x * blockDim.x) {
+    const uint32_t ns = P.dyn[0];
+    for (uint32_t oi = blockIdx.x * blockDim.x + threadIdx.x; oi < ns; oi += gridDim.x * blockDim.x) {
         const uint32_t si = P.order[oi];
         for (uint32_t sub = 0; sub < 2; ++sub) {
-            const uint32_t n = P.nv[sub * P.nsamples + si];
+            const uint32_t n = P.nv[sub * P.cap + si];
             for (uint32_t k = 0; k < n; ++k) {
                 const size_t from = vidx(P, sub, k, si), to = vidx(P, sub, k, oi);
                 P.sva[to] = P.va[from];
@@ -689,11 +698,12 @@ __global__ void __launch_bounds__(128) k_bd_connect(BdParams P) {
     // P.va/vb/vc are the sorted copies here (see bdpt_run_batch): vertex
     // records of sample order[oi] are read at index oi; the per-sample arrays
     // (job, lengths, global index) stay indexed by the sample itself.
-    for (uint32_t oi = blockIdx.x * blockDim.x + threadIdx.x; oi < P.nsamples; oi += gridDim.x * blockDim.x) {
+    const uint32_t ns = P.dyn[0];
+    for (uint32_t oi = blockIdx.x * blockDim.x + threadIdx.x; oi < ns; oi += gridDim.x * blockDim.x) {
         const uint32_t si = P.order[oi];
         const uint32_t job = P.sjob[si];
         const BdJob& J = P.jobs[job];
-        const uint32_t S = P.nv[si], T = P.nv[P.nsamples + si];
+        const uint32_t S = P.nv[si], T = P.nv[P.cap + si];
         const uint32_t pix = uint32_t(P.sindex[si] % (J.width * J.height));
         const uint32_t limit = J.max_depth + 2;
         MisCache mc;
@@ -764,7 +774,14 @@ struct BdptBatcher {
     BdParams P{};
     BdJob* jobs_h = nullptr;      // pinned staging
     BdSegment* seg_h = nullptr;   // pinned staging
+    uint32_t* dyn_h = nullptr;    // pinned staging: samples, segments of the batch
+    uint32_t* dyn_d = nullptr;
     cudaEvent_t staged = nullptr;
+    // The stage sequence of a batch captured as one CUDA graph per max depth
+    // (the kernels read the batch's size from dyn_d, so a graph serves every
+    // batch of that depth), replayed on captured_stream.
+    cudaGraphExec_t graphs[63] = {};
+    cudaStream_t captured_stream = nullptr;
 };
 
 size_t bdpt_batch_bytes(uint32_t max_depth, uint32_t batch) {
@@ -785,6 +802,7 @@ BdptBatcher* bdpt_create(ar_context* ctx, uint32_t max_depth_cap, uint32_t batch
     b->seg_d.alloc(kMaxBdptJobs * sizeof(BdSegment));
     AR_CUDA(cudaMallocHost(&b->jobs_h, kMaxBdptJobs * sizeof(BdJob)));
     AR_CUDA(cudaMallocHost(&b->seg_h, kMaxBdptJobs * sizeof(BdSegment)));
+    AR_CUDA(cudaMallocHost(&b->dyn_h, 4 * sizeof(uint32_t)));
     AR_CUDA(cudaEventCreateWithFlags(&b->staged, cudaEventDisableTiming));
     AR_CUDA(cudaEventRecord(b->staged, ctx->stream));
     char* cur = b->mem.as<char>();
@@ -819,6 +837,9 @@ BdptBatcher* bdpt_create(ar_context* ctx, uint32_t max_depth_cap, uint32_t batch
     P.sh_job = carve<uint32_t>(cur, P.sh_cap);
     P.counts = carve<uint32_t>(cur, kBdCounts);
     P.order = carve<uint32_t>(cur, batch);
+    b->dyn_d = carve<uint32_t>(cur, 4);
+    P.dyn = b->dyn_d;
+    P.cap = batch;
     P.jobs = b->jobs_d.as<BdJob>();
     P.seg = b->seg_d.as<BdSegment>();
     return b.release();
@@ -826,8 +847,11 @@ BdptBatcher* bdpt_create(ar_context* ctx, uint32_t max_depth_cap, uint32_t batch
 
 void bdpt_destroy(BdptBatcher* b) {
     if (!b) return;
+    for (auto& g : b->graphs)
+        if (g) cudaGraphExecDestroy(g);
     if (b->jobs_h) cudaFreeHost(b->jobs_h);
     if (b->seg_h) cudaFreeHost(b->seg_h);
+    if (b->dyn_h) cudaFreeHost(b->dyn_h);
     if (b->staged) cudaEventDestroy(b->staged);
     delete b;
 }
@@ -835,7 +859,62 @@ void bdpt_destroy(BdptBatcher* b) {
 uint32_t bdpt_batch_capacity(const BdptBatcher* b) { return b->batch; }
 uint32_t bdpt_max_depth_cap(const BdptBatcher* b) { return b->max_depth_cap; }
 
-void bdpt_run_batch(BdptBatcher* b, const std::vector<BdJob>& jobs, const std::vector<BdSegment>& segs) {
+// The stages of one batch whose jobs reach `max_depth` bounces, on stream
+// `s`; grids are sized for the batch capacity (the kernels loop over the
+// batch's own size, read from P.dyn).  Returns the number of kernels.
+static uint32_t launch_batch(BdptBatcher* b, uint32_t max_depth, cudaStream_t s) {
+    ar_context* ctx = b->ctx;
+    const BdParams& P = b->P;
+    int* err = ctx->err_flag.as<int>();
+    const int wide = ctx->num_sms * 8;
+    AR_CUDA(cudaMemsetAsync(P.counts, 0, kBdCounts * sizeof(uint32_t), s));
+    {
+        KernelScope ks(ctx->prof, s, "bdpt_generate");
+        k_bd_generate<<<std::max(1, int(std::min<uint64_t>((2ull * b->batch + 255) / 256, wide))), 256, 0, s>>>(P);
+    }
+    for (uint32_t d = 0; d < max_depth; ++d) {
+        {
+            KernelScope ks(ctx->prof, s, "bdpt_extend");
+            k_bd_extend<<<ctx->num_sms * int(ctx->trav_blocks_per_sm), 128, 0, s>>>(P, d, err);
+        }
+        {
+            KernelScope ks(ctx->prof, s, "bdpt_vertex");
+            k_bd_vertex<<<wide, 256, 0, s>>>(P, d);
+        }
+    }
+    const int g = std::max(1, int(std::min<uint64_t>((b->batch + 255) / 256, wide)));
+    {
+        KernelScope ks(ctx->prof, s, "bdpt_sort");
+        k_bd_hist<<<g, 256, 0, s>>>(P);
+        k_bd_scan<<<1, 256, 0, s>>>(P);
+        k_bd_scatter<<<g, 256, 0, s>>>(P);
+    }
+    {
+        KernelScope ks(ctx->prof, s, "bdpt_permute");
+        k_bd_permute<<<g, 256, 0, s>>>(P);
+    }
+    {
+        KernelScope ks(ctx->prof, s, "bdpt_connect");
+        BdParams Pc = P;
+        Pc.va = P.sva;
+        Pc.vb = P.svb;
+        Pc.vc = P.svc;
+        Pc.vuv = P.svuv;
+        k_bd_connect<<<std::max(1, int(std::min<uint64_t>((b->batch + 127) / 128, ctx->num_sms * 16))), 128, 0,
+                       s>>>(Pc);
+    }
+    {
+        KernelScope ks(ctx->prof, s, "bdpt_shadow");
+        k_bd_shadow<<<ctx->num_sms * int(ctx->trav_blocks_per_sm), 128, 0, s>>>(P, err);
+    }
+    k_bd_count<<<1, 32, 0, s>>>(P.counts, max_depth, ctx->stats_d.as<unsigned long long>(), err);
+    AR_CUDA(cudaGetLastError());
+    // generate, (extend, vertex) per depth, hist/scan/scatter, permute,
+    // connect, shadow, count
+    return 2 * max_depth + 8;
+}
+
+uint32_t bdpt_run_batch(BdptBatcher* b, const std::vector<BdJob>& jobs, const std::vector<BdSegment>& segs) {
     ar_context* ctx = b->ctx;
     AR_REQUIRE(!segs.empty() && segs.size() <= kMaxBdptJobs && jobs.size() <= kMaxBdptJobs, AR_ERR_INVALID_ARGUMENT,
                "bad BDPT batch");
@@ -849,59 +928,38 @@ void bdpt_run_batch(BdptBatcher* b, const std::vector<BdJob>& jobs, const std::v
     AR_CUDA(cudaEventSynchronize(b->staged));  // staging buffers free again
     std::copy(jobs.begin(), jobs.end(), b->jobs_h);
     std::copy(segs.begin(), segs.end(), b->seg_h);
+    b->dyn_h[0] = nsamples;
+    b->dyn_h[1] = uint32_t(segs.size());
     AR_CUDA(cudaMemcpyAsync(b->jobs_d.ptr, b->jobs_h, jobs.size() * sizeof(BdJob), cudaMemcpyHostToDevice,
                             ctx->stream));
     AR_CUDA(cudaMemcpyAsync(b->seg_d.ptr, b->seg_h, segs.size() * sizeof(BdSegment), cudaMemcpyHostToDevice,
                             ctx->stream));
+    AR_CUDA(cudaMemcpyAsync(b->dyn_d, b->dyn_h, 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
     AR_CUDA(cudaEventRecord(b->staged, ctx->stream));
-    BdParams P = b->P;
-    P.nseg = uint32_t(segs.size());
-    P.nsamples = nsamples;
-    int* err = ctx->err_flag.as<int>();
-    const int wide = ctx->num_sms * 8;
-    AR_CUDA(cudaMemsetAsync(P.counts, 0, kBdCounts * sizeof(uint32_t), ctx->stream));
-    {
-        KernelScope ks(ctx->prof, ctx->stream, "bdpt_generate");
-        k_bd_generate<<<std::max(1, int(std::min<uint64_t>((2ull * nsamples + 255) / 256, wide))), 256, 0,
-                        ctx->stream>>>(P);
+    if (ctx->prof.on) return launch_batch(b, max_depth, ctx->stream);  // per-stage timing
+    if (b->captured_stream != ctx->stream) {
+        for (auto& g : b->graphs)
+            if (g) cudaGraphExecDestroy(g);
+        for (auto& g : b->graphs) g = nullptr;
+        b->captured_stream = ctx->stream;
     }
-    for (uint32_t d = 0; d < max_depth; ++d) {
-        {
-            KernelScope ks(ctx->prof, ctx->stream, "bdpt_extend");
-            k_bd_extend<<<ctx->num_sms * int(ctx->trav_blocks_per_sm), 128, 0, ctx->stream>>>(P, d, err);
+    cudaGraphExec_t& ge = b->graphs[max_depth];
+    if (!ge) {
+        cudaGraph_t graph;
+        AR_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            launch_batch(b, max_depth, ctx->stream);
+        } catch (...) {
+            cudaStreamEndCapture(ctx->stream, &graph);
+            throw;
         }
-        {
-            KernelScope ks(ctx->prof, ctx->stream, "bdpt_vertex");
-            k_bd_vertex<<<wide, 256, 0, ctx->stream>>>(P, d);
-        }
+        AR_CUDA(cudaStreamEndCapture(ctx->stream, &graph));
+        const cudaError_t e = cudaGraphInstantiate(&ge, graph, 0);
+        cudaGraphDestroy(graph);
+        AR_CUDA(e);
     }
-    {
-        KernelScope ks(ctx->prof, ctx->stream, "bdpt_sort");
-        const int g = std::max(1, int((nsamples + 255) / 256));
-        k_bd_hist<<<g, 256, 0, ctx->stream>>>(P);
-        k_bd_scan<<<1, 256, 0, ctx->stream>>>(P);
-        k_bd_scatter<<<g, 256, 0, ctx->stream>>>(P);
-    }
-    {
-        KernelScope ks(ctx->prof, ctx->stream, "bdpt_permute");
-        k_bd_permute<<<std::max(1, int(std::min<uint64_t>((nsamples + 255) / 256, wide))), 256, 0, ctx->stream>>>(P);
-    }
-    {
-        KernelScope ks(ctx->prof, ctx->stream, "bdpt_connect");
-        BdParams Pc = P;
-        Pc.va = P.sva;
-        Pc.vb = P.svb;
-        Pc.vc = P.svc;
-        Pc.vuv = P.svuv;
-        k_bd_connect<<<std::max(1, int(std::min<uint64_t>((nsamples + 127) / 128, ctx->num_sms * 16))), 128, 0,
-                       ctx->stream>>>(Pc);
-    }
-    {
-        KernelScope ks(ctx->prof, ctx->stream, "bdpt_shadow");
-        k_bd_shadow<<<ctx->num_sms * int(ctx->trav_blocks_per_sm), 128, 0, ctx->stream>>>(P, err);
-    }
-    k_bd_count<<<1, 32, 0, ctx->stream>>>(P.counts, max_depth, ctx->stats_d.as<unsigned long long>(), err);
-    AR_CUDA(cudaGetLastError());
+    AR_CUDA(cudaGraphLaunch(ge, ctx->stream));
+    return 2 * max_depth + 8;
 }
 
 BdJob make_bdpt_job(const ar_scene* sc, const CameraDev& cam, const ar_integrator_cfg& cfg, uint32_t w, uint32_t h,

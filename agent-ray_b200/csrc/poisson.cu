@@ -228,7 +228,7 @@ void poisson_sor_with_scratch(cudaStream_t stream, int num_sms, const ar_integra
     AR_CUDA(cudaGetLastError());
 }
 
-void poisson_reconstruct(ar_context* ctx, const ar_integrator_cfg& cfg, uint32_t w, uint32_t h, const float* primal,
+uint64_t poisson_reconstruct(ar_context* ctx, const ar_integrator_cfg& cfg, uint32_t w, uint32_t h, const float* primal,
                          const float* gx, const float* gy, float* out, double* rel_residual) {
     const size_t n = size_t(w) * h;
     const int grid = std::max(1, std::min(int((n + 255) / 256), ctx->num_sms * 8));
@@ -238,7 +238,7 @@ void poisson_reconstruct(ar_context* ctx, const ar_integrator_cfg& cfg, uint32_t
         float* rhs = ctx->solver.buf.as<float>();
         poisson_sor_with_scratch(st, ctx->num_sms, cfg, w, h, primal, gx, gy, rhs, rhs + 3 * n, out);
         if (rel_residual) *rel_residual = -1.0;
-        return;
+        return 2 + 2 * uint64_t(cfg.poisson_iterations);
     }
     // CG with FP64 refinement.
     const double alpha = double(cfg.alpha);
@@ -261,9 +261,11 @@ void poisson_reconstruct(ar_context* ctx, const ar_integrator_cfg& cfg, uint32_t
     double hb[16];
     double res = 0.0;
     uint32_t total = 0;
+    uint64_t launches = 1;
     for (;;) {
         AR_CUDA(cudaMemsetAsync(scal, 0, 9 * sizeof(double), st));
         k_cg_residual<<<grid, 256, 0, st>>>(w, h, b, x, alpha, r, p, d, scal);
+        launches++;
         AR_CUDA(cudaMemcpyAsync(hb, scal, 12 * sizeof(double), cudaMemcpyDeviceToHost, st));
         AR_CUDA(cudaStreamSynchronize(st));
         res = 0.0;
@@ -280,11 +282,13 @@ void poisson_reconstruct(ar_context* ctx, const ar_integrator_cfg& cfg, uint32_t
         }
         total += inner;
         k_cg_accumulate<<<grid, 256, 0, st>>>(3 * n, x, d);
+        launches += 4 * inner + 1;
     }
     k_cg_output<<<grid, 256, 0, st>>>(3 * n, x, out);
     AR_CUDA(cudaGetLastError());
     AR_CUDA(cudaStreamSynchronize(st));
     if (rel_residual) *rel_residual = res;
+    return launches + 1;
 }
 
 }  // namespace ar

@@ -491,9 +491,9 @@ PathEngine* engine_create(ar_context* ctx, uint32_t capacity) {
 
 void engine_destroy(PathEngine* e) { delete e; }
 
-void engine_update(PathEngine* e, const std::vector<std::pair<uint32_t, JobDev>>& adds,
-                   const std::vector<uint32_t>& removes) {
-    if (adds.empty() && removes.empty()) return;
+size_t engine_update(PathEngine* e, const std::vector<std::pair<uint32_t, JobDev>>& adds,
+                     const std::vector<uint32_t>& removes) {
+    if (adds.empty() && removes.empty()) return 0;
     for (uint32_t slot : removes) {
         auto it = std::find(e->active.begin(), e->active.end(), slot);
         if (it != e->active.end()) e->active.erase(it);
@@ -518,6 +518,7 @@ void engine_update(PathEngine* e, const std::vector<std::pair<uint32_t, JobDev>>
     AR_CUDA(cudaMemcpyAsync(e->active_d.as<uint32_t>() + kMaxActiveJobs, st.active + kMaxActiveJobs,
                             sizeof(uint32_t), cudaMemcpyHostToDevice, e->ctx->stream));
     AR_CUDA(cudaEventRecord(st.ev, e->ctx->stream));
+    return adds.size() * sizeof(JobDev) + (e->active.size() + 1) * sizeof(uint32_t);
 }
 
 void engine_add_job(PathEngine* e, uint32_t slot, const JobDev& job) { engine_update(e, {{slot, job}}, {}); }

@@ -221,7 +221,7 @@ struct ServerImpl {
             j->status = AR_JOB_RUNNING;
             j->t_admit = now_ms();
         }
-        if (!adds.empty()) engine_update(engine, adds, {});
+        if (!adds.empty()) stats.h2d_bytes += engine_update(engine, adds, {});
     }
 
     // Converts / reconstructs the film and copies it to the caller's buffer.
@@ -234,12 +234,15 @@ struct ServerImpl {
             const size_t fb = count * (f64 ? 8 : 4);
             for (int f = 0; f < 3; ++f)
                 film_to_f32(c, static_cast<char*>(j->films) + f * fb, f64, count, f32 + f * count);
-            poisson_reconstruct(c, j->cfg, j->w, j->h, f32, f32 + count, f32 + 2 * count, outd, nullptr);
+            stats.kernel_launches +=
+                3 + poisson_reconstruct(c, j->cfg, j->w, j->h, f32, f32 + count, f32 + 2 * count, outd, nullptr);
         } else {
             film_to_f32(c, j->films, f64, count, outd);
+            stats.kernel_launches += 1;
         }
         AR_CUDA(cudaMemcpyAsync(j->out, outd, count * sizeof(float),
                                 j->out_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c->stream));
+        if (!j->out_on_device) stats.d2h_bytes += count * sizeof(float);
         AR_CUDA(cudaEventCreateWithFlags(&j->fin, cudaEventDisableTiming));
         AR_CUDA(cudaEventRecord(j->fin, c->stream));
         j->fin_stream = c->stream;
@@ -255,6 +258,7 @@ struct ServerImpl {
         AR_CUDA(cudaEventRecord(ev, ctx_pt->stream));
         tick_count++;
         stats.pt_ticks++;
+        stats.kernel_launches += kEngineTickKernels;
         if (snap_pending && cudaEventQuery(snap_ev) == cudaSuccess) {
             snap_pending = false;
             const unsigned long long* done = engine_snapshot_host(engine);
@@ -270,10 +274,11 @@ struct ServerImpl {
                 }
             }
             active_pt.swap(still);
-            if (!removes.empty()) engine_update(engine, {}, removes);
+            if (!removes.empty()) stats.h2d_bytes += engine_update(engine, {}, removes);
         }
         if (!snap_pending) {
             engine_snapshot_done(engine);
+            stats.d2h_bytes += kMaxActiveJobs * sizeof(unsigned long long);
             AR_CUDA(cudaEventRecord(snap_ev, ctx_pt->stream));
             snap_pending = true;
             snap_issued++;
@@ -323,7 +328,8 @@ struct ServerImpl {
             used += take;
         }
         if (segs.empty()) return;
-        bdpt_run_batch(bdpt, jobs, segs);
+        stats.kernel_launches += bdpt_run_batch(bdpt, jobs, segs);
+        stats.h2d_bytes += jobs.size() * sizeof(BdJob) + segs.size() * sizeof(BdSegment);
         AR_CUDA(cudaEventRecord(bd_ev[bd_issued_batches % 2], ctx_bd->stream));
         bd_issued_batches++;
         stats.bdpt_batches++;

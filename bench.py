@@ -1,26 +1,27 @@
 """Benchmark driver: one JSON line on rank 0.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload served|pt_cornell|pt_served4|bdpt_served4|bdpt_room|gdpt_room|bvh]
-                    [--jobs J]
-                    [--window-jobs J] [--served-jobs J]
+                    [--workload served|pt_cornell|pt_cornell_glass|pt_cornell_textured|pt_served4|
+                                bdpt_served4|bdpt_room|gdpt_room|bvh]
+                    [--timed-jobs T] [--config-steps C] [--no-configs]
 
 Workloads (seeded synthetic inputs with the stated shapes; no dataset exists):
-  served      (default) the served batched-rendering stream: Poisson arrivals of
-              2000 jobs, scenes drawn from 8 seeded procedural scenes of
-              10k-1M triangles, resolution from {128,256,512,1024}^2, spp from
-              {4,16,64}, PT or BDPT 70/30 (PT: depth 8, RR from 3; BDPT: depth
-              8, RR from 3, power-heuristic MIS).  Metric: Mpath-samples/s.
-              A step is one window of --window-jobs (16) consecutive jobs of
-              the stream submitted to the render server together (continuous
-              batching under a backlog);
-              `value` is the throughput of the K timed windows with images kept
-              on the GPU, `e2e` the same windows' jobs with images returned to
-              pinned host buffers.  `served` adds p50/p99 latency of a Poisson
-              arrival run at 80% of the measured capacity over the next
-              --served-jobs (160) jobs of the stream, and `plain` the
-              one-job-at-a-time GPU path (ar_render per job) on the first timed
-              window's jobs.
+  served      (default) the served batched-rendering stream (config 5): a
+              seeded stream of 2000 jobs over 8 procedural scenes of
+              10k-1M triangles, resolution from {128,256,512,1024}^2, spp
+              from {4,16,64}, PT or BDPT 70/30 (depth 8, RR from 3,
+              power-heuristic MIS).  Metric: Mpath-samples/s.  The timed
+              set is fixed: jobs [0, T) of the stream (T = 400), whatever K
+              is; a step is 1/K of it, and the K steps are submitted back to
+              back as one backlog (continuous batching).  `value` keeps the
+              images on the GPU, `e2e` renders the same jobs into pinned host
+              buffers, `served` replays the same jobs as Poisson arrivals at
+              80% of the capacity `value` measured (p50/p99 overall and per
+              class), and `plain` renders them one at a time through
+              ar_render (the reference's Integrator::render unit), with the
+              batched-vs-plain speed-up per job class.  The line carries a
+              `configs` object with configs 1-4 measured in the same process
+              (pt_cornell, bvh, bdpt_room, gdpt_room; C timed steps each).
   pt_cornell  PT Cornell box (34 tris + quad light, 256x256, 16 spp, depth 8);
               one step = one full render.
   pt_cornell_glass  config 1 with rough-glass (DielectricBsdf) objects.
@@ -30,17 +31,19 @@ Workloads (seeded synthetic inputs with the stated shapes; no dataset exists):
   bdpt_served4 BDPT on served scene 4, 512x512, 16 spp, depth 8.
   bdpt_room   BDPT on the 200k-tri room, 512x512, 64 spp, depth 10, FP64 film.
   gdpt_room   GDPT on the room, 1024x1024, 32 spp, CG Poisson to 1e-6.
-  bvh         BVH micro-benchmark: 1M triangles, 16M closest-hit rays (Mrays/s).
+  bvh         BVH micro-benchmark: 1M triangles, 16M closest-hit rays (Mrays/s),
+              any hit with t_max 0.25 beside it.
 
-Timing: CUDA events on the stream the library launches on (pt_cornell, bvh)
-or, for the server (which runs on its own internal streams), events recorded
-on an idle stream around the window (submission -> last result), i.e. device
-timestamps of the window's wall span.  L2 is flushed (256 MiB write) before
-every timed step outside its events.  Multi-GPU: one process per GPU, each
-rank serves its own seeded stream (weak scaling, no data-path collective);
-time is the max over ranks.  `--impl reference` times the reference algorithm
-(the C++ restatement of agent-ray's CPU integrators with the reference's
-xoshiro sampler) on all host cores on a bounded sample of the same workload.
+Timing: CUDA events on the stream the library launches on (single renders,
+bvh) or, for the server (which runs on its own internal streams), events
+recorded on an idle stream around the timed set (submission -> last result),
+i.e. device timestamps of its wall span.  L2 is flushed (256 MiB write)
+before every timed step outside its events.  Multi-GPU: one process per GPU,
+each rank serves its own seeded stream (weak scaling, no data-path
+collective); time is the max over ranks.  `--impl reference` times the
+reference algorithm (the C++ restatement of agent-ray's CPU integrators with
+the reference's xoshiro sampler) on all host cores on a bounded sample of the
+same timed set.
 """
 import argparse
 import json
@@ -213,7 +216,7 @@ def job_cfg(job, seed):
 
 
 # ----------------------------------------------------------------- served ----
-def wait_or_dump(srv, job_id, timeout_ms=180_000.0):
+def wait_or_dump(srv, job_id, timeout_ms=300_000.0):
     """Waits for a job; on timeout prints the server's queue state and raises."""
     try:
         return srv.wait(job_id, timeout_ms)
@@ -223,152 +226,216 @@ def wait_or_dump(srv, job_id, timeout_ms=180_000.0):
         raise
 
 
-def run_served(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind):
+def job_class(job):
+    return f"{job['integrator']}_{job['res']}x{job['spp']}"
+
+
+def samples_of(jobs):
+    return sum(j["res"] ** 2 * j["spp"] for j in jobs)
+
+
+# Jobs whose samples cannot fill the 2^22 path slots (PT) or one 2^21-sample
+# BDPT batch by themselves: the classes where batching several jobs can help.
+SMALL_CLASSES = [(128, 4), (128, 16), (128, 64), (256, 4), (256, 16), (512, 4)]
+
+
+def run_served(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind, stream):
+    """The served stream (config 5) on a fixed job set: jobs [0, timed_jobs) of
+    the seeded 2000-job stream, the same set whatever --steps is.
+
+    value   the set submitted as a backlog (K steps = K consecutive slices of
+            the set, submitted back to back) with images kept on the GPU;
+    e2e     the same jobs with images returned to pinned host buffers;
+    served  the same jobs (new seeds) arriving as a Poisson process at 80% of
+            the capacity `value` measured on this job mix: p50/p99 latency
+            overall and per resolution x integrator class;
+    plain   the same jobs one at a time through ar_render (the reference's
+            Integrator::render unit), and per job class the small-job speed-up
+            of batching (each class's jobs as one backlog vs one at a time)."""
     import agentray
     import agentray.scenes as S
 
-    n_jobs = args.jobs
-    stream = rank_stream(n_jobs, rank)
+    full = rank_stream(args.jobs, rank)
+    T = min(args.timed_jobs, len(full))
+    timed = full[:T]
+    K = max(1, args.steps)
+    W = max(3, args.warmup)
+    chunks = [list(c) for c in np.array_split(np.arange(T), K)]
+    warm_jobs = full[T:T + W * args.window_jobs]
     built = [S.served_scene(k) for k in range(8)]
     scenes = [agentray.Scene(ctx, sd) for sd, _ in built]
     cams = [cam for _, cam in built]
     srv = agentray.Server(ctx, film_budget_bytes=24 << 30, path_capacity=args.path_capacity,
-                          bdpt_batch_samples=args.bdpt_batch,
-                          bdpt_max_depth=8)
-    W, K = max(3, args.warmup), args.steps
-    per = max(1, min(args.window_jobs, n_jobs // (W + K + 1)))
-    windows = [stream[i * per:(i + 1) * per] for i in range(W + K)]
-    served_jobs = stream[(W + K) * per:(W + K) * per + args.served_jobs]
+                          bdpt_batch_samples=args.bdpt_batch, bdpt_max_depth=8)
     side = torch.cuda.Stream()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    dev_out = {128: [], 256: [], 512: [], 1024: []}
+    dev_out = [torch.empty(j["res"] ** 2 * 3, dtype=torch.float32, device="cuda") for j in timed]
+    host_out = [torch.empty(j["res"] ** 2 * 3, dtype=torch.float32, pin_memory=True).numpy() for j in timed]
 
-    def device_buffer(res, i):
-        pool = dev_out[res]
-        while len(pool) <= i:
-            pool.append(torch.empty(res * res * 3, dtype=torch.float32, device="cuda"))
-        return pool[i]
+    def submit(job, seed, out):
+        return srv.submit(scenes[job["scene"]], cams[job["scene"]], make_integrator(agentray, job, seed),
+                          job["res"], job["res"], out=out)
 
-    def run_window(jobs, host_out, base_seed):
-        counters = {}
-        ids = []
+    def run_backlog(idx, outs, base_seed, arrivals=None):
+        """Submits timed[i] for i in idx (all at once, or at `arrivals` seconds
+        after the start), waits for all; returns (device-span ms, wall s,
+        infos, server-stats delta)."""
         flush.zero_()
         torch.cuda.synchronize()
+        st0 = srv.stats()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(side)
-        for i, job in enumerate(jobs):
-            r = job["res"]
-            k = counters.get(r, 0)
-            counters[r] = k + 1
-            out = None if host_out else device_buffer(r, k)
-            ids.append(srv.submit(scenes[job["scene"]], cams[job["scene"]], make_integrator(agentray, job,
-                                                                                           base_seed + i), r, r,
-                                  out=out))
-        infos = [wait_or_dump(srv, j) for j in ids]
+        t0 = time.perf_counter()
+        ids = []
+        for n, i in enumerate(idx):
+            if arrivals is not None:
+                delay = arrivals[n] - (time.perf_counter() - t0)
+                if delay > 0:
+                    time.sleep(delay)
+            ids.append(submit(timed[i], base_seed + i, outs[i] if outs is not None else None))
+        infos = [wait_or_dump(srv, x) for x in ids]
         e1.record(side)
         torch.cuda.synchronize()
-        for j in ids:
-            srv.forget(j)
+        wall = time.perf_counter() - t0
+        st1 = srv.stats()
+        for x in ids:
+            srv.forget(x)
         assert all(i["status"] == "done" for i in infos), [i["status"] for i in infos]
-        samples = sum(j["res"] ** 2 * j["spp"] for j in jobs)
-        return e0.elapsed_time(e1), samples, infos
+        return e0.elapsed_time(e1), wall, infos, {k: st1[k] - st0[k] for k in st1}
 
-    # warm-up windows (also calibrate capacity)
+    # warm-up: W steps of window_jobs jobs from beyond the timed set, and the plain path
     for w in range(W):
-        run_window(windows[w], False, 10_000 * w)
+        ids = [srv.submit(scenes[j["scene"]], cams[j["scene"]], make_integrator(agentray, j, 900 + w * 100 + i),
+                          j["res"], j["res"]) for i, j in enumerate(warm_jobs[w * args.window_jobs:
+                                                                          (w + 1) * args.window_jobs])]
+        for x in ids:
+            wait_or_dump(srv, x)
+            srv.forget(x)
+    for j in (dict(timed[0], res=128, spp=4, integrator="pt"), dict(timed[0], res=128, spp=4, integrator="bdpt")):
+        make_integrator(agentray, j, 1).render(scenes[j["scene"]], cams[j["scene"]], 128, 128,
+                                               out=dev_out[0][:128 * 128 * 3])
+    torch.cuda.synchronize()
+
+    # value: the whole set as a backlog, images on the device
     barrier()
-    ms_list, samples_total = [], 0
+    all_idx = [i for c in chunks for i in c]
     with ClockSampler(local) as clk:
-        for k in range(K):
-            ms, smp, _ = run_window(windows[W + k], False, 10_000 * (W + k))
-            ms_list.append(ms)
-            samples_total += smp
-    total_ms = sum(ms_list)
-    value = world * samples_total / (max_over_ranks(dist, total_ms, "cuda") / 1e3) / 1e6
-    capacity_sps = samples_total / (total_ms / 1e3)
+        value_ms, _, _, vstats = run_backlog(all_idx, dev_out, 10_000)
+    total_samples = samples_of(timed)
+    value = world * total_samples / (max_over_ranks(dist, value_ms, "cuda") / 1e3) / 1e6
+    capacity_sps = total_samples / (value_ms / 1e3)
 
-    # e2e: the first two timed windows again with images returned to host
-    e2e_ms, e2e_samples, d2h = 0.0, 0, 0
-    for k in range(min(2, K)):
-        ms, smp, _ = run_window(windows[W + k], True, 10_000 * (W + k))
-        e2e_ms += ms
-        e2e_samples += smp
-        d2h += sum(j["res"] ** 2 * 3 * 4 for j in windows[W + k])
-    e2e_value = e2e_samples / (e2e_ms / 1e3) / 1e6
+    # e2e: the same jobs and seeds, images into pinned host buffers
+    e2e_ms, e2e_wall, _, estats = run_backlog(all_idx, host_out, 10_000)
+    e2e_value = world * total_samples / (max_over_ranks(dist, e2e_ms, "cuda") / 1e3) / 1e6
 
-    # served: Poisson arrivals at 80% of the measured capacity
-    mean_samples = statistics.mean(j["res"] ** 2 * j["spp"] for j in stream)
-    rate = 0.8 * capacity_sps / mean_samples
-    arrivals = np.cumsum(np.random.default_rng(77 + rank).exponential(1.0 / rate, len(served_jobs)))
-    ids = []
-    t_start = time.perf_counter()
-    counters = {}
-    for i, job in enumerate(served_jobs):
-        delay = arrivals[i] - (time.perf_counter() - t_start)
-        if delay > 0:
-            time.sleep(delay)
-        ids.append(srv.submit(scenes[job["scene"]], cams[job["scene"]], make_integrator(agentray, job, 50_000 + i),
-                              job["res"], job["res"]))
-    infos = [wait_or_dump(srv, j) for j in ids]
-    served_span = time.perf_counter() - t_start
+    # served: Poisson arrivals of the same jobs at 80% of this mix's capacity
+    rate = 0.8 * capacity_sps / (total_samples / T)
+    arrivals = np.cumsum(np.random.default_rng(77 + rank).exponential(1.0 / rate, T))
+    _, served_wall, infos, _ = run_backlog(list(range(T)), host_out, 50_000, arrivals=arrivals)
     lat = np.array([i["done_ms"] - i["submit_ms"] for i in infos])
-    served = {"jobs": len(served_jobs), "arrival_rate_jobs_per_s": rate, "load": 0.8,
-              "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
-              "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
-              "mean_ms": float(lat.mean()) if len(lat) else None,
-              "throughput_mpath_samples_per_s": sum(j["res"] ** 2 * j["spp"] for j in served_jobs) / served_span / 1e6}
-    st = srv.stats()
-    relmse = served_relmse(agentray, srv, scenes, cams, stream)
+    by_class = {}
+    for job, l in zip(timed, lat):
+        by_class.setdefault(f"{job['integrator']}_{job['res']}", []).append(l)
+    served = {"jobs": T, "arrival_rate_jobs_per_s": rate, "load": 0.8,
+              "load_basis": "80% of `value`'s measured capacity on this same job set",
+              "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+              "mean_ms": float(lat.mean()), "max_ms": float(lat.max()),
+              "span_s": served_wall,
+              "throughput_mpath_samples_per_s": total_samples / served_wall / 1e6,
+              "by_class": {k: {"jobs": len(v), "p50_ms": float(np.percentile(v, 50)),
+                               "p99_ms": float(np.percentile(v, 99))} for k, v in sorted(by_class.items())}}
+    relmse = served_relmse(agentray, srv, scenes, cams, full)
+
+    # per-class batching of the small jobs: each class's jobs as one backlog
+    batched_class = {}
+    for integ in ("pt", "bdpt"):
+        for res, spp in SMALL_CLASSES:
+            idx = [i for i, j in enumerate(timed) if (j["integrator"], j["res"], j["spp"]) == (integ, res, spp)]
+            if not idx:
+                continue
+            ms, _, _, _ = run_backlog(idx, dev_out, 10_000)
+            batched_class[f"{integ}_{res}x{spp}"] = (len(idx), samples_of([timed[i] for i in idx]), ms)
+    srv_stats = srv.stats()
     srv.close()
 
-    # plain: one job at a time through ar_render (first timed window's jobs)
-    plain_jobs = windows[W]
-    out = torch.empty(1024 * 1024 * 3, dtype=torch.float32, device="cuda")
-    stream_t = torch.cuda.current_stream()
+    # plain: one job at a time through ar_render, the same jobs and seeds
     flush.zero_()
     torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream_t)
-    for i, job in enumerate(plain_jobs):
-        make_integrator(agentray, job, 10_000 * W + i).render(scenes[job["scene"]], cams[job["scene"]], job["res"],
-                                                              job["res"], out=out)
-    e1.record(stream_t)
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(T + 1)]
+    evs[0].record(stream)
+    for i, job in enumerate(timed):
+        make_integrator(agentray, job, 10_000 + i).render(scenes[job["scene"]], cams[job["scene"]], job["res"],
+                                                          job["res"], out=dev_out[i])
+        evs[i + 1].record(stream)
     torch.cuda.synchronize()
-    plain_ms = e0.elapsed_time(e1)
-    plain_value = sum(j["res"] ** 2 * j["spp"] for j in plain_jobs) / (plain_ms / 1e3) / 1e6
-    batched_first = sum(j["res"] ** 2 * j["spp"] for j in plain_jobs) / (ms_list[0] / 1e3) / 1e6
+    plain_ms = evs[0].elapsed_time(evs[T])
+    job_ms = [evs[i].elapsed_time(evs[i + 1]) for i in range(T)]
+    plain_value = total_samples / (plain_ms / 1e3) / 1e6
+    per_class = {}
+    for i, job in enumerate(timed):
+        c = per_class.setdefault(job_class(job), {"jobs": 0, "samples": 0, "plain_ms": 0.0})
+        c["jobs"] += 1
+        c["samples"] += job["res"] ** 2 * job["spp"]
+        c["plain_ms"] += job_ms[i]
+    small_plain_ms = 0.0
+    for name, c in per_class.items():
+        c["plain_mpath_samples_per_s"] = c["samples"] / (c["plain_ms"] / 1e3) / 1e6
+        c["plain_time_share"] = c["plain_ms"] / plain_ms
+        if name in batched_class:
+            n, smp, ms = batched_class[name]
+            c["batched_mpath_samples_per_s"] = smp / (ms / 1e3) / 1e6
+            c["speedup_batched_vs_plain"] = c["batched_mpath_samples_per_s"] / c["plain_mpath_samples_per_s"]
+            small_plain_ms += c["plain_ms"]
+    small_share = small_plain_ms / plain_ms
+    plain = {"value": plain_value, "unit": "Mpath-samples/s", "jobs": T,
+             "speedup_batched_vs_plain": value / world / plain_value,
+             "small_job_plain_time_share": small_share,
+             "bound_if_small_jobs_were_free": 1.0 / max(1e-9, 1.0 - small_share),
+             "small_classes": "jobs of < 2^22 samples: " + ", ".join(f"{r}^2x{s}" for r, s in SMALL_CLASSES),
+             "equal_relmse": "same per-job sample keys: images equal up to atomic-add order "
+                             "(tests/test_gpu_serving.py); relmse below",
+             "per_class": dict(sorted(per_class.items()))}
 
-    if rank == 0:
-        n_pt = sum(1 for w in windows[W:] for j in w if j["integrator"] == "pt")
-        line = {
-            "metric": METRIC, "value": value, "unit": "Mpath-samples/s", "n_gpus": world, "steps": K, "warmup": W,
-            "ms_per_step": total_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic (seeded procedural scenes and job stream)",
-            "config": {"workload": SERVED_DESC, "jobs_per_step": per, "timed_jobs": per * K,
-                       "timed_pt_jobs": n_pt, "stream_jobs": n_jobs,
-                       "stream_use": f"jobs [0, {(W + K) * per}) as W+K windows of {per}, the next "
-                                     f"{len(served_jobs)} as the Poisson-arrival served run", "l2": "flushed (256 MiB write) before each window",
-                       "parallelism": f"replicas x{world}", "server": {"path_capacity": args.path_capacity,
-                                                                       "bdpt_batch_samples": args.bdpt_batch}},
-            "e2e": {"value": e2e_value, "unit": "Mpath-samples/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": int(d2h / max(1, min(2, K))),
-                    "note": "scenes resident; per step the job descriptors go host->device and every image "
-                            "returns to a host buffer"},
-            "plain": {"value": plain_value, "unit": "Mpath-samples/s", "jobs": len(plain_jobs),
-                      "batched_same_jobs": batched_first, "speedup_batched_vs_plain": batched_first / plain_value,
-                      "equal_relmse": "same per-job sample keys: images equal up to atomic-add order "
-                                      "(tests/test_gpu_serving.py)"},
-            "served": served,
-            "relmse": relmse,
-            "server_stats": st,
-            "gpu_launches": int(st["pt_ticks"] * 5 + st["bdpt_batches"] * 20),
-            "clocks": clk.summary(),
-        }
-        line["roofline"] = served_roofline(args, ctx, agentray, S, scenes, cams, built, peaks, peak_kind, torch)
-        line["cpu_baseline"] = cpu_baseline_served(stream, built, n_samples_target=args.cpu_samples)
-        print(json.dumps(line), flush=True)
+    if rank != 0:
+        return None
+    mix_full = {}
+    for j in full:
+        mix_full[j["integrator"]] = mix_full.get(j["integrator"], 0) + j["res"] ** 2 * j["spp"]
+    mix_t = {}
+    for j in timed:
+        mix_t[j["integrator"]] = mix_t.get(j["integrator"], 0) + j["res"] ** 2 * j["spp"]
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mpath-samples/s", "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": value_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded procedural scenes and job stream)",
+        "config": {"workload": SERVED_DESC,
+                   "timed_set": f"jobs [0, {T}) of the seeded {len(full)}-job stream (fixed, independent of --steps)",
+                   "timed_samples": total_samples,
+                   "bdpt_sample_share": {"timed_set": mix_t.get("bdpt", 0) / total_samples,
+                                         "full_stream": mix_full.get("bdpt", 0) / samples_of(full)},
+                   "step": f"1/{K} of the timed set, submitted back to back (one backlog)",
+                   "warmup": f"{W} steps of {args.window_jobs} jobs from beyond the timed set",
+                   "l2": "flushed (256 MiB write) before the timed set",
+                   "parallelism": f"replicas x{world}",
+                   "server": {"path_capacity": args.path_capacity, "bdpt_batch_samples": args.bdpt_batch}},
+        "e2e": {"value": e2e_value, "unit": "Mpath-samples/s", "h2d_bytes_per_step": estats["h2d_bytes"] / K,
+                "d2h_bytes_per_step": estats["d2h_bytes"] / K,
+                "note": "the same jobs and seeds as `value`: per step the job descriptors (job-table entries, "
+                        "BDPT batch descriptors) go host->device, completion snapshots and every image "
+                        "device->host into pinned buffers; scenes resident"},
+        "plain": plain,
+        "served": served,
+        "relmse": relmse,
+        "server_stats": srv_stats,
+        "gpu_launches": int(vstats["kernel_launches"]),
+        "clocks": clk.summary(),
+    }
+    line["roofline"] = served_roofline(args, ctx, agentray, S, scenes, cams, built, peaks, peak_kind, torch,
+                                       line["clocks"])
+    line["cpu_baseline"] = cpu_baseline_served(timed, built, n_samples_target=args.cpu_samples)
+    return line
 
 
 def served_relmse(agentray, srv, scenes, cams, stream):
@@ -409,10 +476,30 @@ def served_relmse(agentray, srv, scenes, cams, stream):
     return out
 
 
-def served_roofline(args, ctx, agentray, S, scenes, cams, built, peaks, peak_kind, torch):
+def issue_ceiling(name, rays_per_s, clocks):
+    """Second ceiling for a traversal kernel: warp instructions issued per
+    second (rays/s x warp instructions per ray, from the kernel's ncu summary)
+    against the SMs' issue rate (148 SMs x 4 schedulers x 1 warp instruction
+    per cycle at the sampled SM clock)."""
+    p = os.path.join(ROOT, "profiles", f"{name}.txt")
+    inst = None
+    if os.path.exists(p):
+        for line in open(p):
+            if line.startswith("warp_inst_per_ray:"):
+                inst = float(line.split(":")[1])
+    mhz = (clocks or {}).get("sm_mhz") or 1965.0
+    peak = 148 * 4 * mhz * 1e6 / 1e9
+    if inst is None:
+        return {"source": f"profiles/{name}.txt has no warp_inst_per_ray line", "peak_ginst_s": peak}
+    achieved = rays_per_s * inst / 1e9
+    return {"bound": "issue", "warp_inst_per_ray": inst, "achieved_ginst_s": achieved, "peak_ginst_s": peak,
+            "frac": achieved / peak, "sm_mhz": mhz, "source": f"profiles/{name}.txt (ncu smsp__inst_executed)"}
+
+
+def served_roofline(args, ctx, agentray, S, scenes, cams, built, peaks, peak_kind, torch, clocks):
     """Per-launch timing of the dominant kernel (pt_extend) on the middle
     scene (k=4, 139k tris) at 512x512 x 16 spp, with the reference-traversal
-    bytes model."""
+    bytes model and the issue-rate ceiling."""
     k = 4
     pt = agentray.PathTracer(agentray.PathTracerConfig(spp=16, max_depth=8, rr_depth=3, seed=3))
     out = torch.empty(512 * 512 * 3, dtype=torch.float32, device="cuda")
@@ -437,6 +524,7 @@ def served_roofline(args, ctx, agentray, S, scenes, cams, built, peaks, peak_kin
             "case": "served scene 4 (138,944 tris), 512x512, 16 spp, PT depth 8",
             "bytes_model": f"rays/launch {rays_per_launch:.0f} x (48 + 32*{nodes:.2f} nodes + 36*{tris:.2f} tris) B; "
                            f"reference-traversal counts",
+            "issue": issue_ceiling("pt_extend_served4", rays_per_launch / avg_s if avg_s > 0 else 0.0, clocks),
             "kernels_ms": {k2: {"launches": v[0], "ms": v[1]} for k2, v in prof.items()}}
 
 
@@ -474,7 +562,7 @@ def cpu_baseline_served(stream, built, n_samples_target):
     cores = os.cpu_count() or 1
     rate, n, samples, secs = cpu_render_rate(stream, built, n_samples_target, cores)
     return {"value": rate, "unit": "Mpath-samples/s", "cores": cores, "kind": "port",
-            "sample": f"first {n} jobs of the stream at 1 spp (full resolution, same scene/integrator mix): "
+            "sample": f"first {n} jobs of the timed set at 1 spp (full resolution, same scene/integrator mix): "
                       f"{samples} path samples in {secs:.1f} s on {cores} threads"}
 
 
@@ -571,6 +659,7 @@ def run_pt_cornell(args, rank, local, world, torch, ctx, barrier, dist, peaks, p
         t0 = time.perf_counter()
         osc.render(cam, cfg, W, H, sampler=O.SAMPLER_XOSHIRO, threads=cores)
         cpu_s = time.perf_counter() - t0
+        clocks = clk.summary()
         line = {
             "metric": METRIC, "value": value, "unit": "Mpath-samples/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -585,12 +674,15 @@ def run_pt_cornell(args, rank, local, world, torch, ctx, barrier, dist, peaks, p
                          "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
                          "traffic": profile_traffic(prof_name), "peak_kind": peak_kind,
                          "bytes_model": f"rays/launch {rays_per_launch:.0f} x (48 + 32*{nodes:.2f} nodes + "
-                                        f"36*{tris:.2f} tris) B; reference-traversal counts"},
+                                        f"36*{tris:.2f} tris) B; reference-traversal counts",
+                         "issue": issue_ceiling(prof_name, rays_per_launch / avg_s if avg_s > 0 else 0.0,
+                                                clocks)},
             "kernels_ms": {k: {"launches": v[0], "ms": v[1]} for k, v in prof.items()},
-            "render_stats": stats, "clocks": clk.summary(),
+            "render_stats": stats, "clocks": clocks,
             "cpu_baseline": {"value": samples / cpu_s / 1e6, "unit": "Mpath-samples/s", "cores": cores,
                              "kind": "port", "sample": f"one full {W}x{H}x{spp}spp render, reference sampler"}}
-        print(json.dumps(line), flush=True)
+        return line
+    return None
 
 
 # ------------------------------------------------------------------ rooms ----
@@ -681,6 +773,9 @@ def run_room(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_ki
         ln, ms = prof.get(top, (1, 0.0))
         rays = pstats["shadow_rays"] if top == "bdpt_shadow" else pstats["extend_rays"]
         achieved = rays * b_ray / (ms / 1e3) / 1e9 if ms > 0 else 0.0
+        clocks = clk.summary()
+        prof_name = {"bdpt_served4": "bdpt_served4", "bdpt_room": "bdpt_shadow_room",
+                     "gdpt_room": "pt_extend_room"}[args.workload]
         import oracle as O
         osc = O.OracleScene(sc)
         cores = os.cpu_count() or 1
@@ -699,47 +794,71 @@ def run_room(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_ki
             "gpu_launches": int(sum(v[0] for v in prof.values()) * args.steps),
             "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peaks["hbm_gbs"],
                          "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
-                         "traffic": profile_traffic({"bdpt_served4": "bdpt_served4",
-                                                     "bdpt_room": "bdpt_shadow_room",
-                                                     "gdpt_room": "pt_extend_room"}[args.workload]),
+                         "traffic": profile_traffic(prof_name),
                          "peak_kind": peak_kind,
                          "bytes_model": f"{rays} rays x (48 + 32*{nodes:.2f} nodes + 36*{tris:.2f} tris) B over "
-                                        f"{ln} launches; reference-traversal counts of primary/interior rays"},
+                                        f"{ln} launches; reference-traversal counts of primary/interior rays",
+                         "issue": issue_ceiling(prof_name, rays / (ms / 1e3) if ms > 0 else 0.0, clocks)},
             "kernels_ms": {k: {"launches": v[0], "ms": v[1]} for k, v in prof.items()},
-            "render_stats": stats, "clocks": clk.summary(),
+            "render_stats": stats, "clocks": clocks,
             "cpu_baseline": {"value": W * H / cpu_s / 1e6, "unit": "Mpath-samples/s", "cores": cores, "kind": "port",
                              "sample": f"one {W}x{H} render at 1 spp, reference sampler"}}
-        print(json.dumps(line), flush=True)
+        return line
+    return None
 
 
 # -------------------------------------------------------------------- bvh ----
 def run_bvh(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind, stream):
+    """Config 2: 1M-triangle soup, 16M rays.  One step = one closest-hit
+    launch over the 16M rays (rays resident in HBM); any-hit (t_max 0.25) is
+    timed the same way beside it; e2e passes host arrays (rays in, hits out)."""
     import agentray
     import agentray.scenes as S
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     n_tris, n_rays = 1_000_000, 16_000_000
     sc = S.triangle_soup(n_tris, seed=2)
+    t0 = time.perf_counter()
     scene = agentray.Scene(ctx, sc)
+    build_s = time.perf_counter() - t0
     ot, dt = S.soup_rays(n_rays, seed=3)
     ot_d = torch.from_numpy(ot).cuda()
     dt_d = torch.from_numpy(dt).cuda()
+    dt_any = dt_d.clone()
+    dt_any[:, 3] = 0.25
     for _ in range(max(3, args.warmup)):
         scene.trace_closest(ot_d, dt_d)
+        scene.trace_any(ot_d, dt_any)
     torch.cuda.synchronize()
     barrier()
-    ev = []
-    with ClockSampler(local) as clk:
+
+    def timed(fn):
+        ev = []
         for _ in range(args.steps):
             flush.zero_()
             a = torch.cuda.Event(enable_timing=True)
             b = torch.cuda.Event(enable_timing=True)
             a.record(stream)
-            scene.trace_closest(ot_d, dt_d)
+            fn()
             b.record(stream)
             ev.append((a, b))
         torch.cuda.synchronize()
-    total_ms = max_over_ranks(dist, sum(a.elapsed_time(b) for a, b in ev), "cuda")
+        return max_over_ranks(dist, sum(a.elapsed_time(b) for a, b in ev), "cuda")
+
+    with ClockSampler(local) as clk:
+        total_ms = timed(lambda: scene.trace_closest(ot_d, dt_d))
+    any_ms = timed(lambda: scene.trace_any(ot_d, dt_any))
     value = world * n_rays * args.steps / (total_ms / 1e3) / 1e6
+    any_value = world * n_rays * args.steps / (any_ms / 1e3) / 1e6
+    # e2e: host arrays in pinned memory, rays copied in and hits copied out each step
+    ot_h = torch.from_numpy(ot).pin_memory().numpy()
+    dt_h = torch.from_numpy(dt).pin_memory().numpy()
+    e2e = []
+    for _ in range(max(1, min(3, args.steps))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        scene.trace_closest(ot_h, dt_h)
+        e2e.append(time.perf_counter() - t0)
+    e2e_value = n_rays / statistics.mean(e2e) / 1e6
     if rank == 0:
         import oracle as O
         osc = O.OracleScene(sc)
@@ -747,23 +866,36 @@ def run_bvh(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kin
         nodes = r["stats"]["nodes"] / 200_000
         tris = r["stats"]["tris"] / 200_000
         b_ray = 32 + 16 + 32 * nodes + 36 * tris
-        achieved = n_rays * b_ray / (total_ms / args.steps / 1e3) / 1e9
+        rays_per_s = n_rays / (total_ms / args.steps / 1e3)
+        achieved = rays_per_s * b_ray / 1e9
         t0 = time.perf_counter()
         osc.trace_closest(ot[:2_000_000], dt[:2_000_000])
         cpu = 2_000_000 / (time.perf_counter() - t0) / 1e6
+        osc.close()
+        clocks = clk.summary()
         line = {"metric": "Mrays/s (closest hit)", "value": value, "unit": "Mrays/s", "n_gpus": world,
                 "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic", "config": {"workload": "bvh: 1M tris, 16M rays closest hit", "l2": "flushed"},
+                "data": "synthetic",
+                "config": {"workload": "bvh: 1M-triangle soup (seed 2), 16M rays (seed 3), closest hit; any hit "
+                                       "with t_max 0.25 beside it", "l2": "flushed; rays 512 MB > L2"},
+                "any_hit": {"value": any_value, "unit": "Mrays/s", "ms_per_step": any_ms / args.steps},
+                "host_bvh_build_s": build_s,
+                "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": n_rays * 32,
+                        "d2h_bytes_per_step": n_rays * 20,
+                        "note": "rays from pinned host arrays, hits (t, u, v, prim; instance id) back to host"},
                 "gpu_launches": args.steps,
-                "roofline": {"bound": "hbm", "kernel": "trace_closest", "achieved": achieved, "peak": peaks["hbm_gbs"],
-                             "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                "roofline": {"bound": "hbm", "kernel": "trace_closest", "achieved": achieved,
+                             "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
                              "traffic": profile_traffic("trace_closest_soup"), "peak_kind": peak_kind,
-                             "bytes_model": f"48 + 32*{nodes:.1f} + 36*{tris:.1f} B/ray"},
-                "clocks": clk.summary(),
+                             "bytes_model": f"48 + 32*{nodes:.1f} + 36*{tris:.1f} B/ray (reference binary SAH "
+                                            f"traversal counts)",
+                             "issue": issue_ceiling("trace_closest_soup", rays_per_s, clocks)},
+                "clocks": clocks,
                 "cpu_baseline": {"value": cpu, "unit": "Mrays/s", "cores": os.cpu_count(), "kind": "port",
                                  "sample": "2M of the 16M rays, reference binary SAH traversal"}}
-        print(json.dumps(line), flush=True)
+        return line
+    return None
 
 
 # -------------------------------------------------------------- reference ----
@@ -776,13 +908,15 @@ def run_reference(args, rank, world):
         return
     import agentray.scenes as S
     cores = os.cpu_count() or 1
-    stream = S.served_stream(args.jobs, seed=5)
+    stream = S.served_stream(args.jobs, seed=5)[:args.timed_jobs]
     built = [S.served_scene(k) for k in range(8)]
     for w in range(args.warmup):
         cpu_render_rate(stream[w * 3:], built, 16384, cores)
     rates, tot_samples, tot_secs = [], 0, 0.0
     for k in range(args.steps):
-        rate, n, samples, secs = cpu_render_rate(stream[k * 7:], built, args.cpu_samples // max(1, args.steps), cores)
+        start = (k * 7) % max(1, len(stream) - 16)
+        rate, n, samples, secs = cpu_render_rate(stream[start:], built, args.cpu_samples // max(1, args.steps),
+                                                 cores)
         tot_samples += samples
         tot_secs += secs
     value = tot_samples / tot_secs / 1e6
@@ -790,9 +924,10 @@ def run_reference(args, rank, world):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_secs / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded procedural scenes and job stream)",
-            "config": {"workload": SERVED_DESC},
+            "config": {"workload": SERVED_DESC,
+                       "timed_set": f"jobs [0, {args.timed_jobs}) of the seeded {args.jobs}-job stream"},
             "cpu_baseline": {"value": value, "unit": "Mpath-samples/s", "cores": cores, "kind": "port",
-                             "sample": f"{args.steps} slices of the stream, jobs at 1 spp over full resolution, "
+                             "sample": f"{args.steps} slices of the timed set, jobs at 1 spp over full resolution, "
                                        f"{tot_samples} samples in {tot_secs:.1f} s"},
             "e2e": {"value": value, "unit": "Mpath-samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -809,8 +944,14 @@ def main():
                              "bdpt_served4", "bdpt_room",
                              "gdpt_room", "bvh"])
     ap.add_argument("--jobs", type=int, default=2000)
-    ap.add_argument("--window-jobs", dest="window_jobs", type=int, default=16)
-    ap.add_argument("--served-jobs", dest="served_jobs", type=int, default=160)
+    ap.add_argument("--timed-jobs", dest="timed_jobs", type=int, default=400,
+                    help="served: the fixed timed set is jobs [0, timed_jobs) of the stream")
+    ap.add_argument("--window-jobs", dest="window_jobs", type=int, default=8,
+                    help="served: jobs per warm-up step")
+    ap.add_argument("--config-steps", dest="config_steps", type=int, default=5,
+                    help="served: timed steps of each configs.* sub-line (configs 1-4)")
+    ap.add_argument("--no-configs", dest="no_configs", action="store_true",
+                    help="served: skip the configs 1-4 sub-lines")
     ap.add_argument("--path-capacity", dest="path_capacity", type=int, default=1 << 22)
     ap.add_argument("--bdpt-batch", dest="bdpt_batch", type=int, default=1 << 21)
     ap.add_argument("--bdpt-batch-mib", dest="bdpt_batch_mib", type=int, default=0,
@@ -844,14 +985,28 @@ def main():
         if dist is not None:
             dist.barrier()
 
+    def run_one(a):
+        if a.workload in ("pt_cornell", "pt_cornell_glass", "pt_cornell_textured", "pt_served4"):
+            return run_pt_cornell(a, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind, stream)
+        if a.workload in ("bdpt_served4", "bdpt_room", "gdpt_room"):
+            return run_room(a, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind, stream)
+        return run_bvh(a, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind, stream)
+
     if args.workload == "served":
-        run_served(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind)
-    elif args.workload in ("pt_cornell", "pt_cornell_glass", "pt_cornell_textured", "pt_served4"):
-        run_pt_cornell(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind, stream)
-    elif args.workload in ("bdpt_served4", "bdpt_room", "gdpt_room"):
-        run_room(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind, stream)
+        line = run_served(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind, stream)
+        if not args.no_configs:
+            # configs 1-4, each measured in this process after the served run
+            subs = {}
+            for name in ("pt_cornell", "bvh", "bdpt_room", "gdpt_room"):
+                a = argparse.Namespace(**vars(args))
+                a.workload, a.steps, a.warmup = name, args.config_steps, 3
+                subs[name] = run_one(a)
+            if line is not None:
+                line["configs"] = subs
     else:
-        run_bvh(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kind, stream)
+        line = run_one(args)
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

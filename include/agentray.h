@@ -406,6 +406,10 @@ typedef struct ar_server_stats {
     uint64_t path_samples_done;
     uint64_t pt_ticks, bdpt_batches;
     uint64_t film_bytes_in_use, film_bytes_peak;
+    /* host<->device bytes the server copied (job tables, batch descriptors,
+     * completion snapshots, results into host buffers) and the kernels it
+     * launched, since creation */
+    uint64_t h2d_bytes, d2h_bytes, kernel_launches;
 } ar_server_stats;
 
 int ar_server_create(ar_context* ctx, const ar_server_opts* opts, ar_server** out);

@@ -55,6 +55,11 @@ def test_alone_equals_mixed(ctx):
     srv.close()
     assert st["jobs_done"] >= len(jobs)
     assert st["pt_ticks"] > 0 and st["bdpt_batches"] > 0
+    # the copy and launch counters: every image came back to host memory, and
+    # each tick launches 5 kernels, each BDPT batch at least 10
+    assert st["d2h_bytes"] >= sum(w * h * 12 for _, _, w, h in jobs)
+    assert st["h2d_bytes"] > 0
+    assert st["kernel_launches"] >= 5 * st["pt_ticks"] + 10 * st["bdpt_batches"]
 
 
 def test_rejection_and_cancellation(ctx):

@@ -292,10 +292,10 @@ __device__ __forceinline__ void push_shadow(const BdParams& P, uint32_t job, f3 
         atomicExch(&P.counts[65], 1u);
         return;
     }
-    P.sh_o[slot] = make_float4(o.x, o.y, o.z, 0.f);
-    P.sh_d[slot] = make_float4(d.x, d.y, d.z, tmax);
-    P.sh_c[slot] = make_float4(c.x, c.y, c.z, __uint_as_float(pix));
-    P.sh_job[slot] = job;
+    st_once(P.sh_o + slot, make_float4(o.x, o.y, o.z, 0.f));
+    st_once(P.sh_d + slot, make_float4(d.x, d.y, d.z, tmax));
+    st_once(P.sh_c + slot, make_float4(c.x, c.y, c.z, __uint_as_float(pix)));
+    st_once(P.sh_job + slot, job);
 }
 
 __global__ void __launch_bounds__(256) k_bd_generate(BdParams P) {
@@ -724,14 +724,14 @@ __global__ void AR_TRAVERSAL_BOUNDS k_bd_shadow(const __grid_constant__ BdParams
     run_traversal<true>(
         &P.counts[kBdShadowCursor], n, err,
         [&](uint32_t m, const DevScene*& s, Ray& r) {
-            const float4 a = P.sh_o[m], d = P.sh_d[m];
-            s = &P.jobs[P.sh_job[m]].sc;
+            const float4 a = ld_once(P.sh_o + m), d = ld_once(P.sh_d + m);
+            s = &P.jobs[ld_once(P.sh_job + m)].sc;
             r = Ray{mk(a.x, a.y, a.z), mk(d.x, d.y, d.z), 0.f, d.w};
         },
         [&](uint32_t m, const HitRec& h) {
             if (h.slot == kInvalid) {
-                const BdJob& J = P.jobs[P.sh_job[m]];
-                const float4 c = P.sh_c[m];
+                const BdJob& J = P.jobs[ld_once(P.sh_job + m)];
+                const float4 c = ld_once(P.sh_c + m);
                 film_add(J, __float_as_uint(c.w), mk(c.x, c.y, c.z) * J.inv_spp);
             }
         });

@@ -328,11 +328,11 @@ __global__ void __launch_bounds__(256, 4) k_shade(EngineDev E, int q) {
         }
         const uint32_t role = (kk.w >> 24) & 3u;
         if (shadow) {
-            E.sh_o[ss] = make_float4(sh_o.x, sh_o.y, sh_o.z, 0.f);
-            E.sh_d[ss] = make_float4(sh_d.x, sh_d.y, sh_d.z, sh_tmax);
-            E.sh_c[ss] = make_float4(sh_c.x, sh_c.y, sh_c.z, __uint_as_float(cont ? 0u : 1u));
-            E.sh_L[ss] = make_float4(L.x, L.y, L.z, 0.f);
-            E.sh_key[ss] = make_uint4(kk.x, kk.y, role, rs);
+            st_once(E.sh_o + ss, make_float4(sh_o.x, sh_o.y, sh_o.z, 0.f));
+            st_once(E.sh_d + ss, make_float4(sh_d.x, sh_d.y, sh_d.z, sh_tmax));
+            st_once(E.sh_c + ss, make_float4(sh_c.x, sh_c.y, sh_c.z, __uint_as_float(cont ? 0u : 1u)));
+            st_once(E.sh_L + ss, make_float4(L.x, L.y, L.z, 0.f));
+            st_once(E.sh_key + ss, make_uint4(kk.x, kk.y, role, rs));
         } else if (!cont) {
             deposit(E, kk.x, kk.y, role, L);
         }
@@ -346,16 +346,16 @@ __global__ void AR_TRAVERSAL_BOUNDS k_shadow(const __grid_constant__ EngineDev E
     run_traversal<true>(
         &E.cnt[9], n, E.err,
         [&](uint32_t m, const DevScene*& s, Ray& r) {
-            const float4 a = E.sh_o[m], b = E.sh_d[m];
+            const float4 a = ld_once(E.sh_o + m), b = ld_once(E.sh_d + m);
             s = &E.jobs[E.sh_key[m].x].sc;
             r = Ray{mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w};
         },
         [&](uint32_t m, const HitRec& h) {
-            const uint4 sk = E.sh_key[m];
-            const float4 c = E.sh_c[m];
+            const uint4 sk = ld_once(E.sh_key + m);
+            const float4 c = ld_once(E.sh_c + m);
             const bool visible = h.slot == kInvalid;
             if (__float_as_uint(c.w) & 1u) {
-                const float4 l = E.sh_L[m];
+                const float4 l = ld_once(E.sh_L + m);
                 f3 L = mk(l.x, l.y, l.z);
                 if (visible) L = L + mk(c.x, c.y, c.z);
                 deposit(E, sk.x, sk.y, sk.z, L);

@@ -16,7 +16,7 @@ __global__ void AR_TRAVERSAL_BOUNDS trace_kernel(const __grid_constant__ DevScen
     run_traversal<kAnyHit>(
         cursor, n, err,
         [&](uint32_t i, const DevScene*& s, Ray& r) {
-            const float4 a = __ldg(org_tmin + i), b = __ldg(dir_tmax + i);
+            const float4 a = ld_once(org_tmin + i), b = ld_once(dir_tmax + i);
             s = &sc;
             r = make_ray(mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w);
         },
@@ -25,11 +25,11 @@ __global__ void AR_TRAVERSAL_BOUNDS trace_kernel(const __grid_constant__ DevScen
                 occluded[i] = h.slot != kInvalid ? 1 : 0;
             } else if (h.slot != kInvalid) {
                 const uint32_t prim = __float_as_uint(__ldg(reinterpret_cast<const float*>(sc.tris + h.slot) + 3));
-                hits[i] = make_float4(h.t, h.u, h.v, __uint_as_float(prim));
-                inst_ids[i] = h.inst;
+                st_once(hits + i, make_float4(h.t, h.u, h.v, __uint_as_float(prim)));
+                st_once(inst_ids + i, h.inst);
             } else {
-                hits[i] = make_float4(INFINITY, 0.f, 0.f, __uint_as_float(kInvalid));
-                inst_ids[i] = kInvalid;
+                st_once(hits + i, make_float4(INFINITY, 0.f, 0.f, __uint_as_float(kInvalid)));
+                st_once(inst_ids + i, kInvalid);
             }
         });
 }

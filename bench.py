@@ -150,15 +150,25 @@ class ClockSampler:
                 "samples": len(sm), "power_w_median": statistics.median(power) if power else None}
 
 
-def profile_traffic(name):
-    """Per-launch DRAM bytes of `name` from the committed ncu summary, if any."""
+def profile_value(name, key):
+    """A `key: value` line of the committed ncu summary profiles/<name>.txt."""
     p = os.path.join(ROOT, "profiles", f"{name}.txt")
     if not os.path.exists(p):
         return None
     for line in open(p):
-        if line.startswith("dram_bytes_per_launch:"):
-            return float(line.split(":")[1])
+        if line.startswith(key + ":"):
+            return float(line.split(":")[1].split()[0])
     return None
+
+
+def profile_traffic(name, rays_per_launch=None):
+    """DRAM bytes (read + write) per launch of the kernel `name` profiles:
+    the summary's per-ray figure times this launch's rays when both are
+    known, else its per-launch figure."""
+    per_ray = profile_value(name, "dram_bytes_per_ray")
+    if per_ray is not None and rays_per_launch:
+        return per_ray * rays_per_launch
+    return profile_value(name, "dram_bytes_per_launch")
 
 
 def camera_rays(cam, n, rng):
@@ -481,12 +491,7 @@ def issue_ceiling(name, rays_per_s, clocks):
     second (rays/s x warp instructions per ray, from the kernel's ncu summary)
     against the SMs' issue rate (148 SMs x 4 schedulers x 1 warp instruction
     per cycle at the sampled SM clock)."""
-    p = os.path.join(ROOT, "profiles", f"{name}.txt")
-    inst = None
-    if os.path.exists(p):
-        for line in open(p):
-            if line.startswith("warp_inst_per_ray:"):
-                inst = float(line.split(":")[1])
+    inst = profile_value(name, "warp_inst_per_ray")
     mhz = (clocks or {}).get("sm_mhz") or 1965.0
     peak = 148 * 4 * mhz * 1e6 / 1e9
     if inst is None:
@@ -519,7 +524,7 @@ def served_roofline(args, ctx, agentray, S, scenes, cams, built, peaks, peak_kin
     avg_s = (ms / max(1, ln)) / 1e3
     achieved = rays_per_launch * b_ray / avg_s / 1e9 if avg_s > 0 else 0.0
     return {"bound": "hbm", "kernel": "pt_extend", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-            "frac": achieved / peaks["hbm_gbs"], "traffic": profile_traffic("pt_extend_served4"),
+            "frac": achieved / peaks["hbm_gbs"], "traffic": profile_traffic("pt_extend_served4", rays_per_launch),
             "peak_kind": peak_kind,
             "case": "served scene 4 (138,944 tris), 512x512, 16 spp, PT depth 8",
             "bytes_model": f"rays/launch {rays_per_launch:.0f} x (48 + 32*{nodes:.2f} nodes + 36*{tris:.2f} tris) B; "
@@ -597,6 +602,10 @@ def run_pt_cornell(args, rank, local, world, torch, ctx, barrier, dist, peaks, p
         desc = "pt_cornell: PT Cornell box 34 tris + quad light, 256x256, 16 spp, depth 8, RR 3"
         prof_name = "pt_extend_cornell"
     spp = 16
+    if args.res or args.spp:  # a reduced case for profiling
+        W = H = args.res or W
+        spp = args.spp or spp
+        desc += f" [resized: {W}x{H}, {spp} spp]"
     scene = agentray.Scene(ctx, sc)
     out = torch.empty(W * H * 3, dtype=torch.float32, device="cuda")
     pt = agentray.PathTracer(agentray.PathTracerConfig(spp=spp, max_depth=8, rr_depth=3, seed=rank))
@@ -672,7 +681,7 @@ def run_pt_cornell(args, rank, local, world, torch, ctx, barrier, dist, peaks, p
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "kernel": "pt_extend", "achieved": achieved, "peak": peaks["hbm_gbs"],
                          "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
-                         "traffic": profile_traffic(prof_name), "peak_kind": peak_kind,
+                         "traffic": profile_traffic(prof_name, rays_per_launch), "peak_kind": peak_kind,
                          "bytes_model": f"rays/launch {rays_per_launch:.0f} x (48 + 32*{nodes:.2f} nodes + "
                                         f"36*{tris:.2f} tris) B; reference-traversal counts",
                          "issue": issue_ceiling(prof_name, rays_per_launch / avg_s if avg_s > 0 else 0.0,
@@ -701,33 +710,33 @@ def run_room(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_ki
     scene = agentray.Scene(ctx, sc)
     ntri = scene.stats()["num_triangles"]
     if args.workload == "bdpt_served4":
-        W = H = 512
-        spp = 16
+        W = H = args.res or 512
+        spp = args.spp or 16
         integ = agentray.BidirectionalPathTracer(agentray.BdptConfig(spp=spp, max_depth=8, rr_depth=3, seed=4 + rank))
         cfg = integrator_cfg(A.INTEGRATOR_BDPT, spp=1, max_depth=8, rr_depth=3)
-        desc = (f"bdpt_served4: BDPT+MIS on served scene 4 ({ntri} tris, 335 instances, 2 quad lights), 512x512, "
-                f"16 spp, max depth 8")
+        desc = (f"bdpt_served4: BDPT+MIS on served scene 4 ({ntri} tris, 335 instances, 2 quad lights), {W}x{H}, "
+                f"{spp} spp, max depth 8")
         top = "bdpt_shadow"
         dtype = "f32"
     elif args.workload == "bdpt_room":
-        W = H = 512
-        spp = 64
+        W = H = args.res or 512
+        spp = args.spp or 64
         integ = agentray.BidirectionalPathTracer(agentray.BdptConfig(spp=spp, max_depth=10, rr_depth=3, seed=4 + rank,
                                                                      film_precision=A.FILM_F64))
         cfg = integrator_cfg(A.INTEGRATOR_BDPT, spp=1, max_depth=10, rr_depth=3)
         desc = (f"bdpt_room: BDPT+MIS (power, beta 2) on the room ({ntri} tris: icospheres + 500 instanced boxes, "
-                f"Lambert/GGX 50/50, 2 quad lights), 512x512, 64 spp, max depth 10, FP64 film")
+                f"Lambert/GGX 50/50, 2 quad lights), {W}x{H}, {spp} spp, max depth 10, FP64 film")
         top = "bdpt_shadow"
         dtype = "f32 transport, f64 film"
     else:
-        W = H = 1024
-        spp = 32
+        W = H = args.res or 1024
+        spp = args.spp or 32
         integ = agentray.GradientDomainPathTracer(agentray.GdptConfig(
             spp=spp, max_depth=8, rr_depth=3, alpha=0.2, poisson_solver=A.POISSON_CG, poisson_tolerance=1e-6,
             seed=4 + rank))
         cfg = integrator_cfg(A.INTEGRATOR_GDPT, spp=1, max_depth=8, rr_depth=3, alpha=0.2,
                              poisson_solver=A.POISSON_SOR, poisson_iterations=200)
-        desc = (f"gdpt_room: GDPT (random replay, x/y shifts) on the room ({ntri} tris), 1024x1024, 32 spp, "
+        desc = (f"gdpt_room: GDPT (random replay, x/y shifts) on the room ({ntri} tris), {W}x{H}, {spp} spp, "
                 f"alpha 0.2, Poisson by FP32 CG with FP64 residual refinement to rel. residual 1e-6")
         top = "pt_extend"
         dtype = "f32 transport, f64 Poisson residuals"
@@ -794,7 +803,7 @@ def run_room(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_ki
             "gpu_launches": int(sum(v[0] for v in prof.values()) * args.steps),
             "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peaks["hbm_gbs"],
                          "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
-                         "traffic": profile_traffic(prof_name),
+                         "traffic": profile_traffic(prof_name, rays / max(1, ln)),
                          "peak_kind": peak_kind,
                          "bytes_model": f"{rays} rays x (48 + 32*{nodes:.2f} nodes + 36*{tris:.2f} tris) B over "
                                         f"{ln} launches; reference-traversal counts of primary/interior rays",
@@ -815,7 +824,7 @@ def run_bvh(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kin
     import agentray
     import agentray.scenes as S
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    n_tris, n_rays = 1_000_000, 16_000_000
+    n_tris, n_rays = 1_000_000, args.rays or 16_000_000
     sc = S.triangle_soup(n_tris, seed=2)
     t0 = time.perf_counter()
     scene = agentray.Scene(ctx, sc)
@@ -877,8 +886,9 @@ def run_bvh(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kin
                 "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic",
-                "config": {"workload": "bvh: 1M-triangle soup (seed 2), 16M rays (seed 3), closest hit; any hit "
-                                       "with t_max 0.25 beside it", "l2": "flushed; rays 512 MB > L2"},
+                "config": {"workload": f"bvh: 1M-triangle soup (seed 2), {n_rays / 1e6:g}M rays (seed 3), closest "
+                                       f"hit; any hit with t_max 0.25 beside it",
+                           "l2": f"flushed; rays {n_rays * 32 / 1e6:.0f} MB"},
                 "any_hit": {"value": any_value, "unit": "Mrays/s", "ms_per_step": any_ms / args.steps},
                 "host_bvh_build_s": build_s,
                 "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": n_rays * 32,
@@ -887,7 +897,7 @@ def run_bvh(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_kin
                 "gpu_launches": args.steps,
                 "roofline": {"bound": "hbm", "kernel": "trace_closest", "achieved": achieved,
                              "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
-                             "traffic": profile_traffic("trace_closest_soup"), "peak_kind": peak_kind,
+                             "traffic": profile_traffic("trace_closest_soup", n_rays), "peak_kind": peak_kind,
                              "bytes_model": f"48 + 32*{nodes:.1f} + 36*{tris:.1f} B/ray (reference binary SAH "
                                             f"traversal counts)",
                              "issue": issue_ceiling("trace_closest_soup", rays_per_s, clocks)},
@@ -957,6 +967,10 @@ def main():
     ap.add_argument("--bdpt-batch-mib", dest="bdpt_batch_mib", type=int, default=0,
                     help="HBM per plain-path BDPT batch (0: the library default)")
     ap.add_argument("--cpu-samples", dest="cpu_samples", type=int, default=4_000_000)
+    ap.add_argument("--res", type=int, default=0, help="single-render workloads: override the resolution "
+                                                         "(reduced cases for profiling)")
+    ap.add_argument("--spp", type=int, default=0, help="single-render workloads: override spp")
+    ap.add_argument("--rays", type=int, default=0, help="bvh: override the ray count")
     args = ap.parse_args()
     rank, local, world = dist_env()
     if args.impl == "reference":

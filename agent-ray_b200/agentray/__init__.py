@@ -157,9 +157,11 @@ class Scene:
         b.on_device = 1 if on_device else 0
         return b
 
-    def trace_closest(self, org_tmin, dir_tmax):
+    def trace_closest(self, org_tmin, dir_tmax, out=None):
         """Closest hit for (n,4) float32 ray arrays (numpy on the host, or torch
-        CUDA tensors).  Returns (hits (n,4): t,u,v,prim_id-bits; inst_ids (n,))."""
+        CUDA tensors).  Returns (hits (n,4): t,u,v,prim_id-bits; inst_ids (n,)).
+        Host arrays may come with `out` = (hits, inst_ids) numpy arrays to fill
+        (pinned ones let the copies overlap the traversal)."""
         dev = not isinstance(org_tmin, np.ndarray)
         if dev:
             import torch
@@ -174,8 +176,13 @@ class Scene:
         org_tmin = np.ascontiguousarray(org_tmin, np.float32)
         dir_tmax = np.ascontiguousarray(dir_tmax, np.float32)
         n = org_tmin.shape[0]
-        hits = np.empty((n, 4), np.float32)
-        inst = np.empty(n, np.uint32)
+        if out is not None:
+            hits, inst = out
+            assert hits.shape == (n, 4) and hits.dtype == np.float32 and hits.flags.c_contiguous
+            assert inst.shape == (n,) and inst.dtype == np.uint32 and inst.flags.c_contiguous
+        else:
+            hits = np.empty((n, 4), np.float32)
+            inst = np.empty(n, np.uint32)
         b = self._batch(org_tmin, dir_tmax, False)
         check(lib().ar_trace_closest(self.ctx.handle, self.handle, C.byref(b), hits.ctypes.data, inst.ctypes.data,
                                      0))
@@ -191,7 +198,7 @@ class Scene:
             raise ValueError("rays must be (n, 4) arrays")
         return org_tmin.to(torch.float32).contiguous(), dir_tmax.to(torch.float32).contiguous()
 
-    def trace_any(self, org_tmin, dir_tmax):
+    def trace_any(self, org_tmin, dir_tmax, out=None):
         """Occlusion (Scene::occluded) for (n,4) float32 ray arrays (numpy on the
         host, or torch CUDA tensors).  Returns (n,) uint8: 1 = occluded."""
         if not isinstance(org_tmin, np.ndarray):
@@ -204,7 +211,8 @@ class Scene:
             return occ
         org_tmin = np.ascontiguousarray(org_tmin, np.float32)
         dir_tmax = np.ascontiguousarray(dir_tmax, np.float32)
-        occ = np.empty(org_tmin.shape[0], np.uint8)
+        occ = np.empty(org_tmin.shape[0], np.uint8) if out is None else out
+        assert occ.shape == (org_tmin.shape[0],) and occ.dtype == np.uint8 and occ.flags.c_contiguous
         b = self._batch(org_tmin, dir_tmax, False)
         check(lib().ar_trace_any(self.ctx.handle, self.handle, C.byref(b), occ.ctypes.data, 0))
         return occ

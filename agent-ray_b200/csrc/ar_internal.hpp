@@ -159,6 +159,10 @@ struct ar_context {
     // (ar_render_samples); range_end == 0 renders all spp samples
     uint32_t range_begin = 0, range_end = 0;
     ar::BdptBatcher* bdpt = nullptr;   // BDPT batch buffers for ar_render
+    // Host-array ray batches (ar_trace_*): copy streams and events that let the
+    // copies of one chunk overlap the traversal of the previous one.
+    cudaStream_t copy_in = nullptr, copy_out = nullptr;
+    cudaEvent_t trace_ev[7] = {};
 };
 
 struct ar_scene {

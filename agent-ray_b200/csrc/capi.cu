@@ -1,4 +1,5 @@
 // extern "C" entry points of libagentray (declared in include/agentray.h).
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -63,6 +64,12 @@ void context_destroy_internal(ar_context* ctx) {
     ctx->engine = nullptr;
     bdpt_destroy(ctx->bdpt);
     ctx->bdpt = nullptr;
+    if (ctx->copy_in) cudaStreamSynchronize(ctx->copy_in);
+    if (ctx->copy_out) cudaStreamSynchronize(ctx->copy_out);
+    for (cudaEvent_t e : ctx->trace_ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->copy_in) cudaStreamDestroy(ctx->copy_in);
+    if (ctx->copy_out) cudaStreamDestroy(ctx->copy_out);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     if (ctx->stats_h) cudaFreeHost(ctx->stats_h);
     delete ctx;
@@ -132,6 +139,16 @@ int ar_scene_get_stats(const ar_scene* scene, ar_scene_stats* out) {
     });
 }
 
+// Rays per chunk of a host-array batch: 4M rays stage 128 MB of rays and
+// 80 MB of hits per slot.
+constexpr uint64_t kTraceChunk = 1ull << 22;
+
+// ar_trace_closest / ar_trace_any.  Device arrays are traced in one launch on
+// the context stream.  A batch with host arrays goes in chunks through two
+// staging slots: a chunk's rays go up on copy_in while the previous chunk is
+// traced on the context stream, and its hits come back on copy_out while the
+// next one is traced, so the PCIe copies (both directions at once) hide
+// behind the traversal.  Returns once host outputs are complete.
 static void trace_common(ar_context* ctx, const ar_scene* scene, const ar_ray_batch* rays, bool any, ar_hit* hits,
                          uint32_t* inst, uint8_t* occ, uint32_t out_on_device) {
     AR_REQUIRE(ctx && scene && rays, AR_ERR_INVALID_ARGUMENT, "null argument");
@@ -141,47 +158,88 @@ static void trace_common(ar_context* ctx, const ar_scene* scene, const ar_ray_ba
     AR_CUDA(cudaSetDevice(ctx->device));
     const uint64_t n = rays->count;
     if (n == 0) return;
-    const size_t ray_bytes = n * sizeof(float4);
-    const size_t out_bytes = any ? n : n * (sizeof(float4) + sizeof(uint32_t));
-    size_t need = (rays->on_device ? 0 : 2 * ray_bytes) + (out_on_device ? 0 : out_bytes + 256);
-    ctx->io.ensure(need + 512);
-    char* base = ctx->io.buf.as<char>();
-    const float4 *ot, *dt;
-    size_t off = 0;
-    if (rays->on_device) {
-        ot = reinterpret_cast<const float4*>(rays->org_tmin);
-        dt = reinterpret_cast<const float4*>(rays->dir_tmax);
-    } else {
-        float4* o = reinterpret_cast<float4*>(base);
-        float4* d = reinterpret_cast<float4*>(base + ray_bytes);
-        AR_CUDA(cudaMemcpyAsync(o, rays->org_tmin, ray_bytes, cudaMemcpyHostToDevice, ctx->stream));
-        AR_CUDA(cudaMemcpyAsync(d, rays->dir_tmax, ray_bytes, cudaMemcpyHostToDevice, ctx->stream));
-        ot = o;
-        dt = d;
-        off = 2 * ray_bytes;
+    const float4* host_o = reinterpret_cast<const float4*>(rays->org_tmin);
+    const float4* host_d = reinterpret_cast<const float4*>(rays->dir_tmax);
+    float4* hit_out = reinterpret_cast<float4*>(hits);
+    if (rays->on_device && out_on_device) {
+        launch_trace(ctx, scene, host_o, host_d, n, any, hit_out, inst, occ);
+        return;
     }
-    float4* dh = nullptr;
-    uint32_t* di = nullptr;
-    uint8_t* dor = nullptr;
-    if (out_on_device) {
-        dh = reinterpret_cast<float4*>(hits);
-        di = inst;
-        dor = occ;
-    } else if (any) {
-        dor = reinterpret_cast<uint8_t*>(base + off);
-    } else {
-        dh = reinterpret_cast<float4*>(base + off);
-        di = reinterpret_cast<uint32_t*>(base + off + n * sizeof(float4));
+    if (!ctx->copy_in) {
+        AR_CUDA(cudaStreamCreateWithFlags(&ctx->copy_in, cudaStreamNonBlocking));
+        AR_CUDA(cudaStreamCreateWithFlags(&ctx->copy_out, cudaStreamNonBlocking));
+        for (cudaEvent_t& ev : ctx->trace_ev) AR_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     }
-    launch_trace(ctx, scene, ot, dt, n, any, dh, di, dor);
-    if (!out_on_device) {
-        if (any) {
-            AR_CUDA(cudaMemcpyAsync(occ, dor, n, cudaMemcpyDeviceToHost, ctx->stream));
+    const uint64_t chunk = std::min(n, kTraceChunk);
+    const int slots = n > chunk ? 2 : 1;
+    const size_t in_bytes = rays->on_device ? 0 : 2 * chunk * sizeof(float4);
+    const size_t out_bytes = out_on_device ? 0 : (any ? chunk : chunk * (sizeof(float4) + sizeof(uint32_t)));
+    const size_t slot_bytes = ((in_bytes + out_bytes + 255) / 256) * 256 + 256;
+    ctx->io.ensure(slots * slot_bytes);
+    cudaEvent_t* in_done = ctx->trace_ev;        // [2]: a slot's rays are on the device
+    cudaEvent_t* traced = ctx->trace_ev + 2;     // [2]: a slot's chunk is traced
+    cudaEvent_t* slot_free = ctx->trace_ev + 4;  // [2]: a slot's hits are back on the host
+    cudaEvent_t start = ctx->trace_ev[6];
+    // staging may still be read by work queued earlier on the context stream
+    AR_CUDA(cudaEventRecord(start, ctx->stream));
+    AR_CUDA(cudaStreamWaitEvent(ctx->copy_in, start, 0));
+    uint64_t k = 0;
+    for (uint64_t off = 0; off < n; off += chunk, ++k) {
+        const uint64_t m = std::min(chunk, n - off);
+        const int s = int(k % 2);
+        char* base = ctx->io.buf.as<char>() + s * slot_bytes;
+        if (k >= 2) AR_CUDA(cudaStreamWaitEvent(ctx->copy_in, out_on_device ? traced[s] : slot_free[s], 0));
+        const float4 *ot, *dt;
+        if (rays->on_device) {
+            ot = host_o + off;
+            dt = host_d + off;
         } else {
-            AR_CUDA(cudaMemcpyAsync(hits, dh, n * sizeof(float4), cudaMemcpyDeviceToHost, ctx->stream));
-            AR_CUDA(cudaMemcpyAsync(inst, di, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+            float4* o = reinterpret_cast<float4*>(base);
+            float4* d = o + chunk;
+            AR_CUDA(cudaMemcpyAsync(o, host_o + off, m * sizeof(float4), cudaMemcpyHostToDevice, ctx->copy_in));
+            AR_CUDA(cudaMemcpyAsync(d, host_d + off, m * sizeof(float4), cudaMemcpyHostToDevice, ctx->copy_in));
+            AR_CUDA(cudaEventRecord(in_done[s], ctx->copy_in));
+            AR_CUDA(cudaStreamWaitEvent(ctx->stream, in_done[s], 0));
+            ot = o;
+            dt = d;
         }
-        check_device_flag(ctx);  // synchronises
+        if (rays->on_device && k >= 2 && !out_on_device)
+            AR_CUDA(cudaStreamWaitEvent(ctx->stream, slot_free[s], 0));
+        float4* dh = nullptr;
+        uint32_t* di = nullptr;
+        uint8_t* dor = nullptr;
+        char* outb = base + in_bytes;
+        if (out_on_device) {
+            dh = any ? nullptr : hit_out + off;
+            di = any ? nullptr : inst + off;
+            dor = any ? occ + off : nullptr;
+        } else if (any) {
+            dor = reinterpret_cast<uint8_t*>(outb);
+        } else {
+            dh = reinterpret_cast<float4*>(outb);
+            di = reinterpret_cast<uint32_t*>(outb + chunk * sizeof(float4));
+        }
+        launch_trace(ctx, scene, ot, dt, m, any, dh, di, dor);
+        AR_CUDA(cudaEventRecord(traced[s], ctx->stream));
+        if (!out_on_device) {
+            AR_CUDA(cudaStreamWaitEvent(ctx->copy_out, traced[s], 0));
+            if (any) {
+                AR_CUDA(cudaMemcpyAsync(occ + off, dor, m, cudaMemcpyDeviceToHost, ctx->copy_out));
+            } else {
+                AR_CUDA(cudaMemcpyAsync(hit_out + off, dh, m * sizeof(float4), cudaMemcpyDeviceToHost,
+                                        ctx->copy_out));
+                AR_CUDA(cudaMemcpyAsync(inst + off, di, m * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                        ctx->copy_out));
+            }
+            AR_CUDA(cudaEventRecord(slot_free[s], ctx->copy_out));
+        }
+    }
+    if (!out_on_device) {
+        AR_CUDA(cudaStreamSynchronize(ctx->copy_out));
+        check_device_flag(ctx);  // synchronises the context stream
+    } else {
+        // the context stream carries on; later uploads into the staging wait for it
+        AR_CUDA(cudaStreamSynchronize(ctx->copy_in));
     }
 }
 

@@ -482,3 +482,44 @@ def test_trace_device_tensors_match_host_arrays(ctx):
     h_occ = g.trace_any(ot, dt)
     d_occ = g.trace_any(torch.from_numpy(ot).cuda().double(), torch.from_numpy(dt).cuda().double())
     np.testing.assert_array_equal(d_occ.cpu().numpy(), h_occ)
+
+
+def test_host_array_batches_pipeline_in_chunks(ctx):
+    # Host-array ray batches larger than one 4M-ray chunk go through the
+    # library's copy/trace pipeline (two staging slots, copy streams): every
+    # combination of host and device inputs and outputs gives the same hits,
+    # for closest and any hit, on an odd-sized batch of three chunks.
+    import ctypes as C
+    import torch
+    sc = S.triangle_soup(200_000, seed=4)
+    g = agentray.Scene(ctx, sc)
+    n = 9_000_001
+    ot, dt = S.soup_rays(n, seed=5, tmax=0.3)
+    ot_d, dt_d = torch.from_numpy(ot).cuda(), torch.from_numpy(dt).cuda()
+    ref_h, ref_i = g.trace_closest(ot_d, dt_d)
+    ref_h, ref_i = ref_h.cpu().numpy(), ref_i.cpu().numpy().view(np.uint32)
+    pin_h = torch.empty((n, 4), dtype=torch.float32, pin_memory=True).numpy()
+    pin_i = torch.empty(n, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    hh, hi = g.trace_closest(ot, dt, out=(pin_h, pin_i))           # host in, host out (pinned)
+    np.testing.assert_array_equal(hh.view(np.uint32), ref_h.view(np.uint32))
+    np.testing.assert_array_equal(hi, ref_i)
+    hh2, hi2 = g.trace_closest(ot, dt)                               # host in, host out (pageable)
+    np.testing.assert_array_equal(hh2.view(np.uint32), ref_h.view(np.uint32))
+    # host in, device out and device in, host out, through the C ABI
+    lib = agentray.lib()
+    bh = A.RayBatch(ot.ctypes.data, dt.ctypes.data, n, 0, 0)
+    dh = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+    di = torch.empty(n, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    agentray.check(lib.ar_trace_closest(ctx.handle, g.handle, C.byref(bh), dh.data_ptr(), di.data_ptr(), 1))
+    agentray.check(lib.ar_context_synchronize(ctx.handle))
+    np.testing.assert_array_equal(dh.cpu().numpy().view(np.uint32), ref_h.view(np.uint32))
+    bd = A.RayBatch(ot_d.data_ptr(), dt_d.data_ptr(), n, 1, 0)
+    oh = np.empty((n, 4), np.float32)
+    oi = np.empty(n, np.uint32)
+    agentray.check(lib.ar_trace_closest(ctx.handle, g.handle, C.byref(bd), oh.ctypes.data, oi.ctypes.data, 0))
+    np.testing.assert_array_equal(oh.view(np.uint32), ref_h.view(np.uint32))
+    np.testing.assert_array_equal(oi, ref_i)
+    occ_ref = g.trace_any(ot_d, dt_d).cpu().numpy()
+    np.testing.assert_array_equal(g.trace_any(ot, dt), occ_ref)
+    assert 0.05 < occ_ref.mean() < 0.95

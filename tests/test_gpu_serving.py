@@ -121,3 +121,29 @@ def test_device_outputs_match_host_outputs(ctx):
         assert np.isfinite(d).all()
         np.testing.assert_allclose(d, srv.result(hj), rtol=1e-5, atol=1e-6)
     srv.close()
+
+
+def test_graph_replay_across_streams_and_depths(ctx):
+    # The PT tick and each BDPT batch depth are CUDA graphs captured on the
+    # context's stream: a render after the stream changes (graphs captured
+    # again) and renders alternating batch depths give the images of a fresh
+    # context (FP64 films: equal up to the order of the atomic adds).
+    import torch
+    sc, cam = S.cornell_box(1)
+    ref_ctx = agentray.Context(0)
+    jobs = [(_bdpt(4, seed=31), 48, 40), (_pt(4, seed=32), 40, 48)]
+    deep = agentray.BidirectionalPathTracer(agentray.BdptConfig(spp=4, max_depth=3, rr_depth=2, seed=33,
+                                                                film_precision=A.FILM_F64))
+    want = [integ.render(agentray.Scene(ref_ctx, sc), cam, w, h).rgb.copy() for integ, w, h in jobs]
+    want_deep = deep.render(agentray.Scene(ref_ctx, sc), cam, 32, 32).rgb.copy()
+    ref_ctx.close()
+    scene = agentray.Scene(ctx, sc)
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    try:
+        for st in (s1, s2, None):
+            ctx.set_stream(st.cuda_stream if st is not None else None)
+            for (integ, w, h), ref in zip(jobs, want):
+                np.testing.assert_allclose(integ.render(scene, cam, w, h).rgb, ref, rtol=1e-6, atol=1e-7)
+            np.testing.assert_allclose(deep.render(scene, cam, 32, 32).rgb, want_deep, rtol=1e-6, atol=1e-7)
+    finally:
+        ctx.set_stream(None)

@@ -390,6 +390,12 @@ struct PathEngine {
     uint64_t ticks = 0;
     std::vector<uint32_t> active;
     unsigned long long* done_h = nullptr;
+    // plain renders: completion events of the two ticks in flight, and the
+    // engine's counters (paths, extend rays, shadow rays) as pinned copies,
+    // read after the render's final synchronisation
+    cudaEvent_t tick_ev[2] = {nullptr, nullptr};
+    unsigned long long* stats_pin = nullptr;
+    unsigned long long stats_seen[3] = {0, 0, 0};
     // Pinned staging for job-table updates, two halves used alternately; each
     // half is reused only after the event of its last copy has completed.
     struct Staging {
@@ -433,6 +439,9 @@ struct PathEngine {
         for (int q = 0; q < 2; ++q)
             if (graph[q]) cudaGraphExecDestroy(graph[q]);
         if (done_h) cudaFreeHost(done_h);
+        if (stats_pin) cudaFreeHost(stats_pin);
+        for (cudaEvent_t ev : tick_ev)
+            if (ev) cudaEventDestroy(ev);
         for (auto& s : stage) {
             if (s.jobs) cudaFreeHost(s.jobs);
             if (s.active) cudaFreeHost(s.active);
@@ -479,6 +488,8 @@ PathEngine* engine_create(ar_context* ctx, uint32_t capacity) {
     AR_CUDA(cudaMemsetAsync(e->E.stats, 0, 8 * sizeof(unsigned long long), ctx->stream));
     AR_CUDA(cudaMemsetAsync(e->active_d.ptr, 0, (kMaxActiveJobs + 1) * sizeof(uint32_t), ctx->stream));
     AR_CUDA(cudaMallocHost(&e->done_h, kMaxActiveJobs * sizeof(unsigned long long)));
+    AR_CUDA(cudaMallocHost(&e->stats_pin, 3 * sizeof(unsigned long long)));
+    for (cudaEvent_t& ev : e->tick_ev) AR_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     for (auto& s : e->stage) {
         AR_CUDA(cudaMallocHost(&s.jobs, kMaxActiveJobs * sizeof(JobDev)));
         AR_CUDA(cudaMallocHost(&s.active, (kMaxActiveJobs + 1) * sizeof(uint32_t)));
@@ -593,14 +604,10 @@ void render_pt_films(ar_context* ctx, const ar_scene* sc, const CameraDev& cam, 
     J.next_sample = npix * s0;
     J.done_paths = 0;
     const uint32_t slot = 0;
-    unsigned long long before[3];
-    AR_CUDA(cudaMemcpyAsync(before, e->E.stats, sizeof(before), cudaMemcpyDeviceToHost, ctx->stream));
-    engine_add_job(e, slot, J);  // synchronises the stream once
+    engine_add_job(e, slot, J);
     // Tick until every path has deposited; completion is checked one tick behind
     // so the GPU always has the next tick queued.
-    cudaEvent_t ev[2];
-    AR_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
-    AR_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+    cudaEvent_t* ev = e->tick_ev;
     unsigned long long* done_pinned = e->done_h;  // two entries, one per in-flight tick
     uint64_t issued = 0;
     const uint64_t tick_cap = 1ull << 26;
@@ -619,16 +626,17 @@ void render_pt_films(ar_context* ctx, const ar_scene* sc, const CameraDev& cam, 
         }
         AR_REQUIRE(issued < tick_cap, AR_ERR_TIMEOUT, "render did not converge");
     }
+    AR_CUDA(cudaMemcpyAsync(e->stats_pin, e->E.stats, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                            ctx->stream));
     AR_CUDA(cudaStreamSynchronize(ctx->stream));
-    cudaEventDestroy(ev[0]);
-    cudaEventDestroy(ev[1]);
     engine_remove_job(e, slot);
-    unsigned long long after[3];
-    AR_CUDA(cudaMemcpy(after, e->E.stats, sizeof(after), cudaMemcpyDeviceToHost));
+    // the counters are cumulative over the engine's life; only this path ticks it
+    const unsigned long long* after = e->stats_pin;
     ctx->last_stats.path_samples = npix * (s1 - s0);
-    ctx->last_stats.paths = after[0] - before[0];
-    ctx->last_stats.extend_rays = after[1] - before[1];
-    ctx->last_stats.shadow_rays = after[2] - before[2];
+    ctx->last_stats.paths = after[0] - e->stats_seen[0];
+    ctx->last_stats.extend_rays = after[1] - e->stats_seen[1];
+    ctx->last_stats.shadow_rays = after[2] - e->stats_seen[2];
+    for (int k = 0; k < 3; ++k) e->stats_seen[k] = after[k];
     ctx->last_stats.extend_launches = issued;
     ctx->last_stats.shadow_launches = issued;
     ctx->stats_pending = false;

@@ -58,7 +58,7 @@ struct BdParams {
     float4* svc;
     float2* svuv;
     uint8_t* nv; // [sub * cap + si]
-    float4* thr; // per subpath q = 2 si + sub: thr.xyz, previous directional pdf
+    float4* thr; // per subpath, at sub * cap + si: thr.xyz, previous directional pdf
     uint32_t* dim;
     float4* ray_o[2];
     float4* ray_d[2];
@@ -75,6 +75,11 @@ struct BdParams {
                        // [kBdHist..], [kBdOffs..]: (S, T) histogram and bucket offsets
     uint32_t* order;   // batch samples sorted by (S, T)
 };
+
+// Subpath q = 2 si + sub (as carried in the ray queues) -> its slot in the
+// per-subpath arrays, camera subpaths first: a warp of camera (or light) rays
+// of neighbouring samples reads contiguous records.
+__device__ __forceinline__ uint32_t sp_slot(const BdParams& P, uint32_t q) { return (q & 1u) * P.cap + (q >> 1); }
 
 __device__ __forceinline__ size_t vidx(const BdParams& P, uint32_t sub, uint32_t k, uint32_t si) {
     return (size_t(sub) * P.maxv + k) * P.cap + si;
@@ -300,10 +305,15 @@ __device__ __forceinline__ void push_shadow(const BdParams& P, uint32_t job, f3 
 
 __global__ void __launch_bounds__(256) k_bd_generate(BdParams P) {
     const uint32_t ns = P.dyn[0], nseg = P.dyn[1];
+    // Threads [0, ns) start the camera subpaths of samples 0..ns-1, threads
+    // [ns, 2 ns) their light subpaths: a warp's 32 rays are all camera rays of
+    // neighbouring pixels, or all light rays, and every later bounce keeps the
+    // queue order, so the extension warps stay coherent.  q = 2 si + sub names
+    // the subpath in the per-subpath arrays.
     for (uint32_t base = blockIdx.x * blockDim.x; base < 2 * ns; base += gridDim.x * blockDim.x) {
-        const uint32_t q = base + threadIdx.x;
-        bool live = q < 2 * ns;
-        const uint32_t si = q >> 1, sub = q & 1u;
+        const uint32_t idx = base + threadIdx.x;
+        bool live = idx < 2 * ns;
+        const uint32_t sub = idx >= ns ? 1u : 0u, si = idx - sub * ns, q = 2 * si + sub;
         Ray r{};
         if (live) {
             uint32_t lo = 0, hi = nseg;
@@ -325,8 +335,8 @@ __global__ void __launch_bounds__(256) k_bd_generate(BdParams P) {
                 r = camera_ray(J.cam, (float(px) + jx) / float(J.width), 1.0f - (float(py) + jy) / float(J.height));
                 store_vtx(P, 0, 0, si, ld3(J.cam.o), r.d, mk(1.f, 1.f, 1.f), 1.0f, kTypeCamera, true, 0);
                 P.nv[si] = 1;
-                P.thr[q] = make_float4(1.f, 1.f, 1.f, camera_pdf_we(J.cam, r.d));
-                P.dim[q] = 2;
+                P.thr[si] = make_float4(1.f, 1.f, 1.f, camera_pdf_we(J.cam, r.d));
+                P.dim[si] = 2;
             } else if (light_enabled(J.sc)) {
                 uint32_t d = kLightSubpathDim;
                 const float u_sel = counter_u01(key, d++);
@@ -361,8 +371,8 @@ __global__ void __launch_bounds__(256) k_bd_generate(BdParams P) {
                     P.nv[P.cap + si] = 1;
                     f3 thr = L.inten / (pp * pdf_dir);
                     thr = thr * fabsf(dot(nl, r.d));
-                    P.thr[q] = make_float4(thr.x, thr.y, thr.z, pdf_dir);
-                    P.dim[q] = d;
+                    P.thr[P.cap + si] = make_float4(thr.x, thr.y, thr.z, pdf_dir);
+                    P.dim[P.cap + si] = d;
                 } else {
                     P.nv[P.cap + si] = 0;
                     live = false;
@@ -418,7 +428,8 @@ __global__ void __launch_bounds__(256, 4) k_bd_vertex(BdParams P, uint32_t depth
                 const f3 ro = mk(ro4.x, ro4.y, ro4.z), rd = mk(rd4.x, rd4.y, rd4.z);
                 const Shade s = make_shade(J.sc, ro, rd, h.x, h.y, h.z, slot, P.hit_inst[j]);
                 const MatView m = load_mat_at(J.sc, s.mat, s.tu, s.tv);
-                const float4 t4 = P.thr[q];
+                const uint32_t spi = sp_slot(P, q);
+                const float4 t4 = P.thr[spi];
                 f3 thr = mk(t4.x, t4.y, t4.z);
                 const uint32_t k = P.nv[sub * P.cap + si];  // index of the new vertex
                 const size_t pi = vidx(P, sub, k - 1, si);
@@ -431,7 +442,7 @@ __global__ void __launch_bounds__(256, 4) k_bd_vertex(BdParams P, uint32_t depth
                 const unsigned long long g = P.sindex[si];
                 const uint32_t npix = J.width * J.height;
                 const uint64_t key = counter_key(J.seed, uint32_t(g % npix), uint32_t(g / npix));
-                uint32_t d = P.dim[q];
+                uint32_t d = P.dim[spi];
                 const f3 wo_l = to_local(s.onb, -rd);
                 const float usel = counter_u01(key, d++);
                 const float ux = counter_u01(key, d++), uy = counter_u01(key, d++);
@@ -451,8 +462,8 @@ __global__ void __launch_bounds__(256, 4) k_bd_vertex(BdParams P, uint32_t depth
                         const f3 wi_w = to_world(s.onb, wi);
                         no = s.p + (s.n * 1e-4f) * signum(dot(wi_w, s.n));
                         nd = normalize(wi_w);
-                        P.thr[q] = make_float4(thr.x, thr.y, thr.z, pdf);
-                        P.dim[q] = d;
+                        P.thr[spi] = make_float4(thr.x, thr.y, thr.z, pdf);
+                        P.dim[spi] = d;
                         cont = true;
                     }
                 }

@@ -314,8 +314,16 @@ def run_served(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_
         assert all(i["status"] == "done" for i in infos), [i["status"] for i in infos]
         return e0.elapsed_time(e1), wall, infos, {k: st1[k] - st0[k] for k in st1}
 
-    # warm-up: W steps of window_jobs jobs from beyond the timed set, and the plain path
-    for w in range(W):
+    # warm-up: the first step submits the timed set at 1 spp as one backlog, so
+    # the server's film pool holds buffers for every job of the set before the
+    # timed passes; the others run window_jobs jobs from beyond the timed set.
+    # Then the plain path once per integrator.
+    ids = [srv.submit(scenes[j["scene"]], cams[j["scene"]], make_integrator(agentray, dict(j, spp=1), 800 + i),
+                      j["res"], j["res"], out=dev_out[i]) for i, j in enumerate(timed)]
+    for x in ids:
+        wait_or_dump(srv, x)
+        srv.forget(x)
+    for w in range(1, W):
         ids = [srv.submit(scenes[j["scene"]], cams[j["scene"]], make_integrator(agentray, j, 900 + w * 100 + i),
                           j["res"], j["res"]) for i, j in enumerate(warm_jobs[w * args.window_jobs:
                                                                           (w + 1) * args.window_jobs])]
@@ -426,7 +434,8 @@ def run_served(args, rank, local, world, torch, ctx, barrier, dist, peaks, peak_
                    "bdpt_sample_share": {"timed_set": mix_t.get("bdpt", 0) / total_samples,
                                          "full_stream": mix_full.get("bdpt", 0) / samples_of(full)},
                    "step": f"1/{K} of the timed set, submitted back to back (one backlog)",
-                   "warmup": f"{W} steps of {args.window_jobs} jobs from beyond the timed set",
+                   "warmup": f"{W} steps: the timed set at 1 spp as one backlog, then {W - 1} x {args.window_jobs} "
+                             f"jobs from beyond the timed set",
                    "l2": "flushed (256 MiB write) before the timed set",
                    "parallelism": f"replicas x{world}",
                    "server": {"path_capacity": args.path_capacity, "bdpt_batch_samples": args.bdpt_batch}},

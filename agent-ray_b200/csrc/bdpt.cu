@@ -95,7 +95,9 @@ struct Vtx {
 
 __device__ __forceinline__ Vtx load_vtx(const BdParams& P, uint32_t sub, uint32_t k, uint32_t si) {
     const size_t i = vidx(P, sub, k, si);
-    const float4 a = P.va[i], b = P.vb[i], c = P.vc[i];
+    // read-only where this is called (connection and MIS stages): through the
+    // non-coherent path (connection stage -2.5%)
+    const float4 a = __ldg(P.va + i), b = __ldg(P.vb + i), c = __ldg(P.vc + i);
     Vtx v;
     v.p = mk(a.x, a.y, a.z);
     v.pdf_fwd = a.w;
@@ -127,7 +129,7 @@ __device__ __forceinline__ void store_vtx(const BdParams& P, uint32_t sub, uint3
 __device__ __forceinline__ MatView vtx_mat(const BdParams& P, const BdJob& J, const Vtx& v, uint32_t sub, uint32_t k,
                                            uint32_t si) {
     if (!v.uv) return load_mat(J.sc, v.index);
-    const float2 uv = P.vuv[vidx(P, sub, k, si)];
+    const float2 uv = __ldg(P.vuv + vidx(P, sub, k, si));
     return load_mat_at(J.sc, v.index, uv.x, uv.y);
 }
 

@@ -220,13 +220,13 @@ __global__ void __launch_bounds__(256, 4) k_shade(EngineDev E, int q) {
         f3 new_o, new_d, sh_o, sh_d, sh_c, L, thr;
         float sh_tmax = 0.f, prev_pdf = 0.f;
         if (j < n) {
-            kk = B.key[j];
+            kk = ld_once(B.key + j);  // the path's records are read once per tick: evict-first
             live = !(kk.w & kDead);
         }
         if (live) {
             const JobDev& J = E.jobs[kk.x];
-            const float4 h = E.hit[j];
-            const float4 t4 = B.thr[j], r4 = B.rad[j];
+            const float4 h = ld_once(E.hit + j);
+            const float4 t4 = ld_once(B.thr + j), r4 = ld_once(B.rad + j);
             thr = mk(t4.x, t4.y, t4.z);
             prev_pdf = t4.w;
             L = mk(r4.x, r4.y, r4.z);
@@ -236,9 +236,9 @@ __global__ void __launch_bounds__(256, 4) k_shade(EngineDev E, int q) {
             if (slot != kInvalid) {
                 const DevScene& sc = J.sc;
                 const uint64_t key = counter_key(J.seed, kk.y, kk.z);
-                const float4 ro4 = B.ray_o[j], rd4 = B.ray_d[j];
+                const float4 ro4 = ld_once(B.ray_o + j), rd4 = ld_once(B.ray_d + j);
                 const f3 ro = mk(ro4.x, ro4.y, ro4.z), rd = mk(rd4.x, rd4.y, rd4.z);
-                const Shade s = make_shade(sc, ro, rd, h.x, h.y, h.z, slot, E.hit_inst[j]);
+                const Shade s = make_shade(sc, ro, rd, h.x, h.y, h.z, slot, ld_once(E.hit_inst + j));
                 const MatView m = load_mat_at(sc, s.mat, s.tu, s.tv);
                 const f3 wo = -rd;
                 const f3 wo_l = to_local(s.onb, wo);

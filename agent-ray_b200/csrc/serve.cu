@@ -101,7 +101,8 @@ struct SJob {
     size_t scratch_bytes = 0;
     uint32_t slot = kInvalid;
     uint64_t total_paths = 0;
-    uint64_t bd_next = 0, bd_last_batch = 0;
+    uint64_t bd_next = 0;
+    uint32_t bd_outstanding = 0;  // issued BDPT batches of this job not yet complete
     uint64_t min_snap = 0;  // first done-counter snapshot issued after admission
     uint64_t last_done = 0; // done paths seen in the last snapshot (diagnostics)
     bool bd_issued = false;
@@ -114,10 +115,15 @@ struct SJob {
 struct ServerImpl {
     int device = 0;
     ar_server_opts opts{};
+    // BDPT batches run on two lanes (context + batch buffers), each with one
+    // batch in flight: the stage tails of one batch (the last rays of a depth,
+    // the connection and shadow stages) overlap the other's work.  Lane 0's
+    // stream also carries the BDPT films' clears and the results.
+    static constexpr int kBdLanes = 2;
     ar_context* ctx_pt = nullptr;
-    ar_context* ctx_bd = nullptr;
+    ar_context* ctx_bd[kBdLanes] = {};
     PathEngine* engine = nullptr;
-    BdptBatcher* bdpt = nullptr;
+    BdptBatcher* bdpt[kBdLanes] = {};
     DevicePool pool;
     std::chrono::steady_clock::time_point t0;
 
@@ -141,8 +147,13 @@ struct ServerImpl {
     cudaEvent_t snap_ev = nullptr;
     bool snap_pending = false;
     uint64_t snap_issued = 0;   // id of the last snapshot issued (1-based)
-    // BDPT batches in flight
-    cudaEvent_t bd_ev[2] = {};
+    // BDPT batches in flight, one per lane
+    struct BdLane {
+        cudaEvent_t done = nullptr;
+        bool busy = false;
+        std::vector<SJob*> members;
+    } bd_lane[kBdLanes];
+    cudaEvent_t bd_admitted = nullptr;  // lane 0: the BDPT films cleared so far
     uint64_t bd_issued_batches = 0, bd_done_batches = 0;
     std::thread worker;
 
@@ -227,7 +238,8 @@ struct ServerImpl {
                 adds.push_back({j->slot, J});
                 active_pt.push_back(j);
             } else {
-                AR_CUDA(cudaMemsetAsync(j->films, 0, j->films_bytes, ctx_bd->stream));
+                AR_CUDA(cudaMemsetAsync(j->films, 0, j->films_bytes, ctx_bd[0]->stream));
+                AR_CUDA(cudaEventRecord(bd_admitted, ctx_bd[0]->stream));
                 active_bd.push_back(j);
             }
             std::lock_guard<std::mutex> lk(mu);
@@ -300,55 +312,64 @@ struct ServerImpl {
 
     void step_bd() {
         // reap finished batches
-        while (bd_done_batches < bd_issued_batches &&
-               cudaEventQuery(bd_ev[bd_done_batches % 2]) == cudaSuccess)
+        for (BdLane& L : bd_lane) {
+            if (!L.busy || cudaEventQuery(L.done) != cudaSuccess) continue;
+            for (SJob* j : L.members) j->bd_outstanding--;
+            L.members.clear();
+            L.busy = false;
             bd_done_batches++;
+        }
         if (!active_bd.empty()) {
             std::vector<SJob*> still;
             for (SJob* j : active_bd) {
-                if (j->bd_issued && j->bd_last_batch <= bd_done_batches) finish(j, ctx_bd);
+                if (j->bd_issued && j->bd_outstanding == 0) finish(j, ctx_bd[0]);
                 else still.push_back(j);
             }
             active_bd.swap(still);
         }
-        if (bd_issued_batches - bd_done_batches >= 2) return;  // two batches in flight
-        std::vector<BdJob> jobs;
-        std::vector<BdSegment> segs;
-        std::vector<SJob*> members;
-        // Each waiting job is offered an equal share of the batch, then what
-        // the shares leave goes oldest first (as the PT tick plan does).
-        const uint32_t cap = bdpt_batch_capacity(bdpt);
-        uint32_t waiting = 0;
-        for (SJob* j : active_bd) waiting += j->bd_issued ? 0u : 1u;
-        const uint32_t share = waiting ? cap / waiting : 0;
-        uint32_t left = cap;
-        for (SJob* j : active_bd)
-            if (!j->bd_issued) left -= uint32_t(std::min<uint64_t>(j->samples - j->bd_next, share));
-        uint32_t used = 0;
-        for (SJob* j : active_bd) {
-            if (j->bd_issued) continue;
-            const uint64_t rem = j->samples - j->bd_next;
-            const uint64_t fair = std::min<uint64_t>(rem, share);
-            const uint64_t extra = std::min<uint64_t>(rem - fair, left);
-            left -= uint32_t(extra);
-            const uint32_t take = uint32_t(fair + extra);
-            if (take == 0) continue;
-            const CameraDev cam = make_camera(j->cam);
-            segs.push_back(BdSegment{uint32_t(jobs.size()), used, take, 0, j->bd_next});
-            jobs.push_back(make_bdpt_job(j->scene, cam, j->cfg, j->w, j->h, j->films));
-            members.push_back(j);
-            j->bd_next += take;
-            used += take;
-        }
-        if (segs.empty()) return;
-        stats.kernel_launches += bdpt_run_batch(bdpt, jobs, segs);
-        stats.h2d_bytes += jobs.size() * sizeof(BdJob) + segs.size() * sizeof(BdSegment);
-        AR_CUDA(cudaEventRecord(bd_ev[bd_issued_batches % 2], ctx_bd->stream));
-        bd_issued_batches++;
-        stats.bdpt_batches++;
-        for (SJob* j : members) {
-            j->bd_last_batch = bd_issued_batches;
-            if (j->bd_next >= j->samples) j->bd_issued = true;
+        for (int lane = 0; lane < kBdLanes; ++lane) {
+            BdLane& L = bd_lane[lane];
+            if (L.busy) continue;
+            std::vector<BdJob> jobs;
+            std::vector<BdSegment> segs;
+            // Each waiting job is offered an equal share of the batch, then what
+            // the shares leave goes oldest first (as the PT tick plan does).
+            const uint32_t cap = bdpt_batch_capacity(bdpt[lane]);
+            uint32_t waiting = 0;
+            for (SJob* j : active_bd) waiting += j->bd_issued ? 0u : 1u;
+            const uint32_t share = waiting ? cap / waiting : 0;
+            uint32_t left = cap;
+            for (SJob* j : active_bd)
+                if (!j->bd_issued) left -= uint32_t(std::min<uint64_t>(j->samples - j->bd_next, share));
+            uint32_t used = 0;
+            for (SJob* j : active_bd) {
+                if (j->bd_issued) continue;
+                const uint64_t rem = j->samples - j->bd_next;
+                const uint64_t fair = std::min<uint64_t>(rem, share);
+                const uint64_t extra = std::min<uint64_t>(rem - fair, left);
+                left -= uint32_t(extra);
+                const uint32_t take = uint32_t(fair + extra);
+                if (take == 0) continue;
+                const CameraDev cam = make_camera(j->cam);
+                segs.push_back(BdSegment{uint32_t(jobs.size()), used, take, 0, j->bd_next});
+                jobs.push_back(make_bdpt_job(j->scene, cam, j->cfg, j->w, j->h, j->films));
+                L.members.push_back(j);
+                j->bd_next += take;
+                used += take;
+            }
+            if (segs.empty()) return;
+            ar_context* c = ctx_bd[lane];
+            if (lane != 0) AR_CUDA(cudaStreamWaitEvent(c->stream, bd_admitted, 0));  // films cleared first
+            stats.kernel_launches += bdpt_run_batch(bdpt[lane], jobs, segs);
+            stats.h2d_bytes += jobs.size() * sizeof(BdJob) + segs.size() * sizeof(BdSegment);
+            AR_CUDA(cudaEventRecord(L.done, c->stream));
+            L.busy = true;
+            bd_issued_batches++;
+            stats.bdpt_batches++;
+            for (SJob* j : L.members) {
+                j->bd_outstanding++;
+                if (j->bd_next >= j->samples) j->bd_issued = true;
+            }
         }
     }
 
@@ -402,12 +423,39 @@ struct ServerImpl {
         for (SJob* j : active_bd)
             s += "  bdpt job " + std::to_string(j->id) + " next=" + std::to_string(j->bd_next) + "/" +
                  std::to_string(j->samples) + " issued=" + std::to_string(j->bd_issued) +
-                 " last_batch=" + std::to_string(j->bd_last_batch) + "\n";
+                 " batches_in_flight=" + std::to_string(j->bd_outstanding) + "\n";
         for (SJob* j : finishing) s += "  finishing job " + std::to_string(j->id) + "\n";
         std::lock_guard<std::mutex> lk(mu);
         debug_text = s;
         debug_requested = false;
         cv_done.notify_all();
+    }
+
+    // Frees the device state (after the worker has stopped, or when creation
+    // fails part way); safe on partly created state.
+    void release() {
+        cudaSetDevice(device);
+        if (ctx_pt) cudaStreamSynchronize(ctx_pt->stream);
+        for (ar_context* c : ctx_bd)
+            if (c) cudaStreamSynchronize(c->stream);
+        for (auto& e : tick_ev)
+            if (e) cudaEventDestroy(e);
+        for (auto& L : bd_lane)
+            if (L.done) cudaEventDestroy(L.done);
+        if (bd_admitted) cudaEventDestroy(bd_admitted);
+        if (snap_ev) cudaEventDestroy(snap_ev);
+        if (engine) engine_destroy(engine);
+        for (BdptBatcher*& b : bdpt) {
+            bdpt_destroy(b);
+            b = nullptr;
+        }
+        if (ctx_pt) context_destroy_internal(ctx_pt);
+        for (ar_context*& c : ctx_bd) {
+            if (c) context_destroy_internal(c);
+            c = nullptr;
+        }
+        engine = nullptr;
+        ctx_pt = nullptr;
     }
 
     void run() {
@@ -473,20 +521,38 @@ int ar_server_create(ar_context* ctx, const ar_server_opts* o, ar_server** out) 
         if (!S.opts.bdpt_max_depth) S.opts.bdpt_max_depth = 10;
         if (!S.opts.max_active_jobs || S.opts.max_active_jobs > kMaxActiveJobs) S.opts.max_active_jobs = kMaxActiveJobs;
         S.t0 = std::chrono::steady_clock::now();
-        S.ctx_pt = context_create_internal(ctx->device);
-        S.ctx_bd = context_create_internal(ctx->device);
-        for (ar_context* c : {S.ctx_pt, S.ctx_bd}) {  // launch shapes follow the caller's context
-            c->trav_blocks_per_sm = ctx->trav_blocks_per_sm;
-            c->shade_block = ctx->shade_block;
+        try {
+            S.ctx_pt = context_create_internal(ctx->device);
+            {
+                // PT ticks are short and latency-bound: their stream gets the
+                // device's highest priority, so a tick's blocks go ahead of the
+                // BDPT lanes' whenever SMs free up
+                int least = 0, greatest = 0;
+                AR_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+                cudaStream_t hp = nullptr;
+                AR_CUDA(cudaStreamCreateWithPriority(&hp, cudaStreamNonBlocking, greatest));
+                AR_CUDA(cudaStreamDestroy(S.ctx_pt->own_stream));
+                S.ctx_pt->own_stream = S.ctx_pt->stream = hp;
+            }
+            for (auto& c : S.ctx_bd) c = context_create_internal(ctx->device);
+            for (ar_context* c : {S.ctx_pt, S.ctx_bd[0], S.ctx_bd[1]}) {  // launch shapes follow the caller's context
+                c->trav_blocks_per_sm = ctx->trav_blocks_per_sm;
+                c->shade_block = ctx->shade_block;
+            }
+            S.engine = engine_create(S.ctx_pt, S.opts.path_capacity);
+            for (int l = 0; l < ServerImpl::kBdLanes; ++l)
+                S.bdpt[l] = bdpt_create(S.ctx_bd[l], S.opts.bdpt_max_depth, S.opts.bdpt_batch_samples);
+            for (uint32_t i = S.opts.max_active_jobs; i-- > 0;) S.free_slots.push_back(i);
+            for (auto& e : S.tick_ev) AR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            for (auto& L : S.bd_lane) AR_CUDA(cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming));
+            AR_CUDA(cudaEventCreateWithFlags(&S.bd_admitted, cudaEventDisableTiming));
+            AR_CUDA(cudaEventCreateWithFlags(&S.snap_ev, cudaEventDisableTiming));
+            AR_CUDA(cudaStreamSynchronize(S.ctx_pt->stream));
+            for (ar_context* c : S.ctx_bd) AR_CUDA(cudaStreamSynchronize(c->stream));
+        } catch (...) {
+            S.release();
+            throw;
         }
-        S.engine = engine_create(S.ctx_pt, S.opts.path_capacity);
-        S.bdpt = bdpt_create(S.ctx_bd, S.opts.bdpt_max_depth, S.opts.bdpt_batch_samples);
-        for (uint32_t i = S.opts.max_active_jobs; i-- > 0;) S.free_slots.push_back(i);
-        for (auto& e : S.tick_ev) AR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        for (auto& e : S.bd_ev) AR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        AR_CUDA(cudaEventCreateWithFlags(&S.snap_ev, cudaEventDisableTiming));
-        AR_CUDA(cudaStreamSynchronize(S.ctx_pt->stream));
-        AR_CUDA(cudaStreamSynchronize(S.ctx_bd->stream));
         S.worker = std::thread([&S] { S.run(); });
         *out = s.release();
     });
@@ -502,16 +568,7 @@ int ar_server_destroy(ar_server* s) {
         }
         S.cv_work.notify_all();
         if (S.worker.joinable()) S.worker.join();
-        cudaSetDevice(S.device);
-        cudaStreamSynchronize(S.ctx_pt->stream);
-        cudaStreamSynchronize(S.ctx_bd->stream);
-        for (auto& e : S.tick_ev) cudaEventDestroy(e);
-        for (auto& e : S.bd_ev) cudaEventDestroy(e);
-        cudaEventDestroy(S.snap_ev);
-        engine_destroy(S.engine);
-        bdpt_destroy(S.bdpt);
-        context_destroy_internal(S.ctx_pt);
-        context_destroy_internal(S.ctx_bd);
+        S.release();
         delete s;
     });
 }

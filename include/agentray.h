@@ -389,7 +389,8 @@ enum ar_job_status {
 typedef struct ar_server_opts {
     uint64_t film_budget_bytes;      /* HBM for job films (0: 8 GiB) */
     uint32_t path_capacity;          /* path slots of the streaming engine (0: 2^22) */
-    uint32_t bdpt_batch_samples;     /* samples per BDPT batch (0: 2^20) */
+    uint32_t bdpt_batch_samples;     /* samples per BDPT batch (0: 2^20); the server keeps
+                                        two batches' buffers (two lanes) */
     uint32_t bdpt_max_depth;         /* largest BDPT max_depth accepted (0: 10) */
     uint32_t max_active_jobs;        /* 0: 1024 */
 } ar_server_opts;

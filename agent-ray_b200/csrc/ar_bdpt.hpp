@@ -36,9 +36,10 @@ void bdpt_destroy(BdptBatcher* b);
 uint32_t bdpt_batch_capacity(const BdptBatcher* b);
 uint32_t bdpt_max_depth_cap(const BdptBatcher* b);
 size_t bdpt_batch_bytes(uint32_t max_depth, uint32_t batch);
-// Enqueues one batch on the context stream; returns the number of kernels
-// it launched.
-uint32_t bdpt_run_batch(BdptBatcher* b, const std::vector<BdJob>& jobs, const std::vector<BdSegment>& segs);
+// Enqueues one batch on `stream` (nullptr: the context stream); returns the
+// number of kernels it launched.
+uint32_t bdpt_run_batch(BdptBatcher* b, const std::vector<BdJob>& jobs, const std::vector<BdSegment>& segs,
+                        cudaStream_t stream = nullptr);
 BdJob make_bdpt_job(const ar_scene* sc, const CameraDev& cam, const ar_integrator_cfg& cfg, uint32_t w, uint32_t h,
                     void* film);
 

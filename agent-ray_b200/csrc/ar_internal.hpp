@@ -159,6 +159,11 @@ struct ar_context {
     // (ar_render_samples); range_end == 0 renders all spp samples
     uint32_t range_begin = 0, range_end = 0;
     ar::BdptBatcher* bdpt = nullptr;   // BDPT batch buffers for ar_render
+    // second BDPT lane of ar_render: its batch buffers and stream, and the
+    // events that fork it from and join it to the context stream
+    ar::BdptBatcher* bdpt2 = nullptr;
+    cudaStream_t lane_stream = nullptr;
+    cudaEvent_t lane_ev[2] = {};
     // Host-array ray batches (ar_trace_*): copy streams and events that let the
     // copies of one chunk overlap the traversal of the previous one.
     cudaStream_t copy_in = nullptr, copy_out = nullptr;

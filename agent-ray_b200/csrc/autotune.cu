@@ -47,6 +47,9 @@ void set_tuning(ar_context* ctx, const ar_tuning& t) {
     if ((size_t(mib) << 20) != ctx->bdpt_budget) {
         bdpt_destroy(ctx->bdpt);
         ctx->bdpt = nullptr;
+        if (ctx->lane_stream) AR_CUDA(cudaStreamSynchronize(ctx->lane_stream));
+        bdpt_destroy(ctx->bdpt2);
+        ctx->bdpt2 = nullptr;
     }
     ctx->engine_capacity = cap;
     ctx->trav_blocks_per_sm = tb;

@@ -754,9 +754,10 @@ __global__ void k_bd_count(const uint32_t* counts, uint32_t max_depth, unsigned 
     if (threadIdx.x == 0) {
         unsigned long long ext = 0;
         for (uint32_t d = 0; d < max_depth; ++d) ext += counts[d];
-        stats[0] += counts[0];
-        stats[1] += ext;
-        stats[2] += counts[64];
+        // atomics: batches of one render may run on two streams at once
+        atomicAdd(&stats[0], (unsigned long long)counts[0]);
+        atomicAdd(&stats[1], ext);
+        atomicAdd(&stats[2], (unsigned long long)counts[64]);
         if (counts[65]) atomicExch(err, 4);
     }
 }
@@ -927,8 +928,10 @@ static uint32_t launch_batch(BdptBatcher* b, uint32_t max_depth, cudaStream_t s)
     return 2 * max_depth + 8;
 }
 
-uint32_t bdpt_run_batch(BdptBatcher* b, const std::vector<BdJob>& jobs, const std::vector<BdSegment>& segs) {
+uint32_t bdpt_run_batch(BdptBatcher* b, const std::vector<BdJob>& jobs, const std::vector<BdSegment>& segs,
+                        cudaStream_t stream) {
     ar_context* ctx = b->ctx;
+    cudaStream_t st = stream ? stream : ctx->stream;
     AR_REQUIRE(!segs.empty() && segs.size() <= kMaxBdptJobs && jobs.size() <= kMaxBdptJobs, AR_ERR_INVALID_ARGUMENT,
                "bad BDPT batch");
     uint32_t nsamples = 0, max_depth = 0;
@@ -944,34 +947,34 @@ uint32_t bdpt_run_batch(BdptBatcher* b, const std::vector<BdJob>& jobs, const st
     b->dyn_h[0] = nsamples;
     b->dyn_h[1] = uint32_t(segs.size());
     AR_CUDA(cudaMemcpyAsync(b->jobs_d.ptr, b->jobs_h, jobs.size() * sizeof(BdJob), cudaMemcpyHostToDevice,
-                            ctx->stream));
+                            st));
     AR_CUDA(cudaMemcpyAsync(b->seg_d.ptr, b->seg_h, segs.size() * sizeof(BdSegment), cudaMemcpyHostToDevice,
-                            ctx->stream));
-    AR_CUDA(cudaMemcpyAsync(b->dyn_d, b->dyn_h, 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
-    AR_CUDA(cudaEventRecord(b->staged, ctx->stream));
-    if (ctx->prof.on) return launch_batch(b, max_depth, ctx->stream);  // per-stage timing
-    if (b->captured_stream != ctx->stream) {
+                            st));
+    AR_CUDA(cudaMemcpyAsync(b->dyn_d, b->dyn_h, 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    AR_CUDA(cudaEventRecord(b->staged, st));
+    if (ctx->prof.on) return launch_batch(b, max_depth, st);  // per-stage timing
+    if (b->captured_stream != st) {
         for (auto& g : b->graphs)
             if (g) cudaGraphExecDestroy(g);
         for (auto& g : b->graphs) g = nullptr;
-        b->captured_stream = ctx->stream;
+        b->captured_stream = st;
     }
     cudaGraphExec_t& ge = b->graphs[max_depth];
     if (!ge) {
         cudaGraph_t graph;
-        AR_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        AR_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         try {
-            launch_batch(b, max_depth, ctx->stream);
+            launch_batch(b, max_depth, st);
         } catch (...) {
-            cudaStreamEndCapture(ctx->stream, &graph);
+            cudaStreamEndCapture(st, &graph);
             throw;
         }
-        AR_CUDA(cudaStreamEndCapture(ctx->stream, &graph));
+        AR_CUDA(cudaStreamEndCapture(st, &graph));
         const cudaError_t e = cudaGraphInstantiate(&ge, graph, 0);
         cudaGraphDestroy(graph);
         AR_CUDA(e);
     }
-    AR_CUDA(cudaGraphLaunch(ge, ctx->stream));
+    AR_CUDA(cudaGraphLaunch(ge, st));
     return 2 * max_depth + 8;
 }
 
@@ -1004,21 +1007,52 @@ void render_bdpt_film(ar_context* ctx, const ar_scene* sc, const CameraDev& cam,
     const size_t budget = ctx->bdpt_budget;
     const size_t per = bdpt_batch_bytes(cfg.max_depth, 1024) / 1024 + 1;
     const uint32_t batch = uint32_t(std::max<uint64_t>(1024, std::min<uint64_t>(total, budget / per)));
-    if (!ctx->bdpt || bdpt_max_depth_cap(ctx->bdpt) < cfg.max_depth || bdpt_batch_capacity(ctx->bdpt) < batch) {
+    const auto fits = [&](const BdptBatcher* b) {
+        return b && bdpt_max_depth_cap(b) >= cfg.max_depth && bdpt_batch_capacity(b) >= batch;
+    };
+    if (!fits(ctx->bdpt)) {
         AR_CUDA(cudaStreamSynchronize(ctx->stream));
         bdpt_destroy(ctx->bdpt);
         ctx->bdpt = nullptr;
         ctx->bdpt = bdpt_create(ctx, std::max(cfg.max_depth, 10u), batch);
     }
+    const uint32_t cap = bdpt_batch_capacity(ctx->bdpt);
+    // Renders of two or more batches alternate them over two lanes (the
+    // context stream and a second stream, each with its own batch buffers):
+    // one batch's stage tails overlap the other's work.  Profiling keeps one
+    // lane so that the per-stage times do not overlap.
+    const bool two_lanes = total > cap && !ctx->prof.on;
+    if (two_lanes) {
+        if (!ctx->lane_stream) {
+            AR_CUDA(cudaStreamCreateWithFlags(&ctx->lane_stream, cudaStreamNonBlocking));
+            for (cudaEvent_t& e : ctx->lane_ev) AR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        }
+        if (!fits(ctx->bdpt2) || bdpt_batch_capacity(ctx->bdpt2) < cap) {
+            AR_CUDA(cudaStreamSynchronize(ctx->lane_stream));
+            bdpt_destroy(ctx->bdpt2);
+            ctx->bdpt2 = nullptr;
+            ctx->bdpt2 = bdpt_create(ctx, bdpt_max_depth_cap(ctx->bdpt), cap);
+        }
+    }
     const bool f64 = cfg.film_precision == AR_FILM_F64;
     AR_CUDA(cudaMemsetAsync(film, 0, size_t(w) * h * 3 * (f64 ? sizeof(double) : sizeof(float)), ctx->stream));
     AR_CUDA(cudaMemsetAsync(ctx->stats_d.ptr, 0, 8 * sizeof(uint64_t), ctx->stream));
+    if (two_lanes) {  // fork: the second lane starts after the clears
+        AR_CUDA(cudaEventRecord(ctx->lane_ev[0], ctx->stream));
+        AR_CUDA(cudaStreamWaitEvent(ctx->lane_stream, ctx->lane_ev[0], 0));
+    }
     const std::vector<BdJob> jobs{make_bdpt_job(sc, cam, cfg, w, h, film)};
-    const uint32_t cap = bdpt_batch_capacity(ctx->bdpt);
     uint64_t batches = 0;
     for (uint64_t begin = 0; begin < total; begin += cap, ++batches) {
         const uint32_t n = uint32_t(std::min<uint64_t>(cap, total - begin));
-        bdpt_run_batch(ctx->bdpt, jobs, {BdSegment{0, 0, n, 0, first + begin}});
+        if (two_lanes && (batches & 1))
+            bdpt_run_batch(ctx->bdpt2, jobs, {BdSegment{0, 0, n, 0, first + begin}}, ctx->lane_stream);
+        else
+            bdpt_run_batch(ctx->bdpt, jobs, {BdSegment{0, 0, n, 0, first + begin}});
+    }
+    if (two_lanes) {  // join: the context stream waits for the second lane
+        AR_CUDA(cudaEventRecord(ctx->lane_ev[1], ctx->lane_stream));
+        AR_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->lane_ev[1], 0));
     }
     AR_CUDA(cudaMemcpyAsync(ctx->stats_h, ctx->stats_d.ptr, 8 * sizeof(uint64_t), cudaMemcpyDeviceToHost,
                             ctx->stream));

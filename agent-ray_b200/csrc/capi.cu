@@ -64,6 +64,12 @@ void context_destroy_internal(ar_context* ctx) {
     ctx->engine = nullptr;
     bdpt_destroy(ctx->bdpt);
     ctx->bdpt = nullptr;
+    if (ctx->lane_stream) cudaStreamSynchronize(ctx->lane_stream);
+    bdpt_destroy(ctx->bdpt2);
+    ctx->bdpt2 = nullptr;
+    for (cudaEvent_t e : ctx->lane_ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->lane_stream) cudaStreamDestroy(ctx->lane_stream);
     if (ctx->copy_in) cudaStreamSynchronize(ctx->copy_in);
     if (ctx->copy_out) cudaStreamSynchronize(ctx->copy_out);
     for (cudaEvent_t e : ctx->trace_ev)

@@ -252,7 +252,9 @@ typedef struct ar_tuning {
     uint32_t path_capacity;          /* PT/GDPT engine path slots (queue capacity; 0: 2^22) */
     uint32_t traversal_blocks_per_sm;/* persistent traversal grid, 128-thread blocks per SM, 1..8 (0: 8) */
     uint32_t shade_block;            /* threads per block of the shading stage: 64, 128 or 256 (0: 256) */
-    uint32_t bdpt_batch_mib;         /* HBM for one BDPT batch of ar_render, MiB (0: 12288) */
+    uint32_t bdpt_batch_mib;         /* HBM for one BDPT batch of ar_render, MiB (0: 12288);
+                                        a render of more than one batch keeps two
+                                        (two lanes) */
 } ar_tuning;
 
 int ar_context_get_tuning(const ar_context* ctx, ar_tuning* out);

@@ -169,15 +169,51 @@ __device__ __forceinline__ RayPre precompute(f3 o, f3 d, float tmin) {
 }
 
 __device__ __forceinline__ uint32_t byte_of(uint32_t w, uint32_t i) { return (w >> (8 * i)) & 0xffu; }
-// Byte i of w as a float, exactly: the bits 0x4B0000qq encode 2^23 + qq, and
-// subtracting 2^23 is exact (a byte-permute and an add instead of an I2F).
-__device__ __forceinline__ float byte_to_float(uint32_t w, uint32_t i) {
-    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7650u + i)) - 8388608.0f;
+// Packed pairs of f32 (Blackwell's f32x2 arithmetic: one instruction per
+// pair, each half rounded exactly as the scalar instruction would).
+__device__ __forceinline__ uint64_t f2_pack(float lo, float hi) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void f2_unpack(uint64_t v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ uint64_t f2_fma(uint64_t a, uint64_t b, uint64_t c) {
+    uint64_t r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+__device__ __forceinline__ uint64_t f2_add(uint64_t a, uint64_t b) {
+    uint64_t r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+// max / min of three (NaN operands ignored, as fmaxf / fminf do)
+__device__ __forceinline__ float fmax3(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+__device__ __forceinline__ float fmin3(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+// Byte j of w as the float 2^23 + byte: the bits 0x4B0000qq encode 2^23 + qq,
+// and subtracting 2^23 afterwards is exact (a byte-permute and an add
+// instead of an I2F).
+__device__ __forceinline__ float biased_byte(uint32_t w, uint32_t j) {
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7650u + j));
 }
 
 // Intersects the 8 children of node `ni`.  Outputs the node group (bits 8..15:
 // internal-child hits in traversal order i, bits 0..7: imask) and the leaf
-// primitive hit mask relative to tri_base.
+// primitive hit mask relative to tri_base.  Each child's six slab distances
+// come from three packed multiply-adds, each half the scalar
+// fmaf(byte, a, b) of the same operands (measured against the scalar form:
+// served-scene traversal stages -2%, two children per pair instead of the
+// (x, y) / (near z, far z) pairs used here: -0.3..+0.5%, more spills).
 __device__ __forceinline__ void intersect_node(const WideNode* nodes, uint32_t ni, const RayPre& r, float tmax,
                                                uint32_t& child_base, uint32_t& node_bits, uint32_t& tri_base,
                                                uint32_t& tri_bits) {
@@ -192,6 +228,9 @@ __device__ __forceinline__ void intersect_node(const WideNode* nodes, uint32_t n
     const float bx = (px - r.o.x) * r.inv.x;
     const float by = (py - r.o.y) * r.inv.y;
     const float bz = (pz - r.o.z) * r.inv.z;
+    // pairs: (x, y) of the near and of the far planes, and (near z, far z)
+    const uint64_t AXY = f2_pack(ax, ay), BXY = f2_pack(bx, by), AZZ = f2_pack(az, az), BZZ = f2_pack(bz, bz);
+    const uint64_t UNBIAS = f2_pack(-8388608.0f, -8388608.0f);
     child_base = w1.x;
     tri_base = w1.y;
     // near/far plane bytes per axis, chosen by the ray octant
@@ -208,14 +247,12 @@ __device__ __forceinline__ void intersect_node(const WideNode* nodes, uint32_t n
         const uint32_t nzw = nz ? hiz : loz, fzw = nz ? loz : hiz;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            const float tnx = fmaf(byte_to_float(nxw, j), ax, bx);
-            const float tfx = fmaf(byte_to_float(fxw, j), ax, bx);
-            const float tny = fmaf(byte_to_float(nyw, j), ay, by);
-            const float tfy = fmaf(byte_to_float(fyw, j), ay, by);
-            const float tnz = fmaf(byte_to_float(nzw, j), az, bz);
-            const float tfz = fmaf(byte_to_float(fzw, j), az, bz);
-            const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, r.tmin));
-            const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tfar_limit));
+            float tnx, tny, tfx, tfy, tnz, tfz;
+            f2_unpack(f2_fma(f2_add(f2_pack(biased_byte(nxw, j), biased_byte(nyw, j)), UNBIAS), AXY, BXY), tnx, tny);
+            f2_unpack(f2_fma(f2_add(f2_pack(biased_byte(fxw, j), biased_byte(fyw, j)), UNBIAS), AXY, BXY), tfx, tfy);
+            f2_unpack(f2_fma(f2_add(f2_pack(biased_byte(nzw, j), biased_byte(fzw, j)), UNBIAS), AZZ, BZZ), tnz, tfz);
+            const float tn = fmax3(tnx, tny, fmaxf(tnz, r.tmin));
+            const float tf = fmin3(tfx, tfy, fminf(tfz, tfar_limit));
             const uint32_t s = uint32_t(half * 4 + j);
             if (tn <= tf) {
                 const uint32_t m = byte_of(meta, j);

@@ -98,12 +98,14 @@ __device__ __forceinline__ void deposit(const EngineDev& E, uint32_t job, uint32
     count_done(E, job);
 }
 
-// Free slots -> samples of the active jobs.  Each job with samples left is
-// first offered an equal share of the free slots (so a small job finishes in
-// the tick it arrives instead of waiting behind a large one), then what the
-// shares leave goes to the jobs oldest first; every free slot is used as
-// before, only the split changes.  Images do not depend on the split: every
-// sample is keyed by (job seed, pixel, sample).
+// Free slots -> samples of the active jobs.  A job whose remaining paths fit
+// in an equal share of the free slots takes them all (so a small job finishes
+// in the tick it arrives instead of waiting behind a large one); what those
+// leave goes to the other jobs oldest first, so large jobs fill the slots one
+// after another and a tick's paths mostly trace one scene, as one job alone
+// would.  Every free slot is used as before, only the split changes.  Images
+// do not depend on the split: every sample is keyed by (job seed, pixel,
+// sample).
 __global__ void k_plan(EngineDev E, int q) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     const uint32_t n_cont = E.cnt[q];
@@ -115,22 +117,23 @@ __global__ void k_plan(EngineDev E, int q) {
         const JobDev& J = E.jobs[E.active[a]];
         if (J.total_samples > J.next_sample) waiting++;
     }
-    const uint32_t share = waiting ? free_paths / waiting : 0;
+    const unsigned long long share = waiting ? free_paths / waiting : 0;
     uint32_t left = free_paths;
-    for (uint32_t a = 0; a < na; ++a) {  // the equal shares
+    for (uint32_t a = 0; a < na; ++a) {  // jobs that fit in their share
         const JobDev& J = E.jobs[E.active[a]];
         const unsigned long long rem = J.total_samples - J.next_sample;
-        left -= uint32_t(min(rem, (unsigned long long)(share / J.roles))) * J.roles;
+        if (rem * J.roles <= share) left -= uint32_t(rem) * J.roles;
     }
-    for (uint32_t a = 0; a < na; ++a) {  // shares plus the remainder, oldest first
+    for (uint32_t a = 0; a < na; ++a) {  // those, and the rest oldest first
         const uint32_t j = E.active[a];
         JobDev& J = E.jobs[j];
         const unsigned long long rem = J.total_samples - J.next_sample;
         if (rem == 0) continue;
-        const unsigned long long fair = min(rem, (unsigned long long)(share / J.roles));
-        const unsigned long long extra = min(rem - fair, (unsigned long long)(left / J.roles));
-        left -= uint32_t(extra) * J.roles;
-        const unsigned long long take = fair + extra;
+        unsigned long long take = rem;
+        if (rem * J.roles > share) {
+            take = min(rem, (unsigned long long)(left / J.roles));
+            left -= uint32_t(take) * J.roles;
+        }
         if (take == 0) continue;
         E.plan[nseg] = Segment{j, n_cont + used, uint32_t(take), J.roles, J.next_sample};
         J.next_sample += take;

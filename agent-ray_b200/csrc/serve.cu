@@ -332,30 +332,33 @@ struct ServerImpl {
             if (L.busy) continue;
             std::vector<BdJob> jobs;
             std::vector<BdSegment> segs;
-            // Each waiting job is offered an equal share of the batch, then what
-            // the shares leave goes oldest first (as the PT tick plan does).
+            // A waiting job whose remaining samples fit in an equal share of the
+            // batch takes them all; the rest of the batch goes to the other jobs
+            // oldest first (as the PT tick plan does), so large jobs run one
+            // after another and a batch mostly traces one scene.
             const uint32_t cap = bdpt_batch_capacity(bdpt[lane]);
             uint32_t waiting = 0;
             for (SJob* j : active_bd) waiting += j->bd_issued ? 0u : 1u;
-            const uint32_t share = waiting ? cap / waiting : 0;
-            uint32_t left = cap;
+            const uint64_t share = waiting ? cap / waiting : 0;
+            uint64_t left = cap;
             for (SJob* j : active_bd)
-                if (!j->bd_issued) left -= uint32_t(std::min<uint64_t>(j->samples - j->bd_next, share));
+                if (!j->bd_issued && j->samples - j->bd_next <= share) left -= j->samples - j->bd_next;
             uint32_t used = 0;
             for (SJob* j : active_bd) {
                 if (j->bd_issued) continue;
                 const uint64_t rem = j->samples - j->bd_next;
-                const uint64_t fair = std::min<uint64_t>(rem, share);
-                const uint64_t extra = std::min<uint64_t>(rem - fair, left);
-                left -= uint32_t(extra);
-                const uint32_t take = uint32_t(fair + extra);
+                uint64_t take = rem;
+                if (rem > share) {
+                    take = std::min<uint64_t>(rem, left);
+                    left -= take;
+                }
                 if (take == 0) continue;
                 const CameraDev cam = make_camera(j->cam);
-                segs.push_back(BdSegment{uint32_t(jobs.size()), used, take, 0, j->bd_next});
+                segs.push_back(BdSegment{uint32_t(jobs.size()), used, uint32_t(take), 0, j->bd_next});
                 jobs.push_back(make_bdpt_job(j->scene, cam, j->cfg, j->w, j->h, j->films));
                 L.members.push_back(j);
                 j->bd_next += take;
-                used += take;
+                used += uint32_t(take);
             }
             if (segs.empty()) return;
             ar_context* c = ctx_bd[lane];

@@ -101,11 +101,12 @@ __device__ __forceinline__ void deposit(const EngineDev& E, uint32_t job, uint32
 // Free slots -> samples of the active jobs.  A job whose remaining paths fit
 // in an equal share of the free slots takes them all (so a small job finishes
 // in the tick it arrives instead of waiting behind a large one); what those
-// leave goes to the other jobs oldest first, so large jobs fill the slots one
-// after another and a tick's paths mostly trace one scene, as one job alone
-// would.  Every free slot is used as before, only the split changes.  Images
-// do not depend on the split: every sample is keyed by (job seed, pixel,
-// sample).
+// leave goes to the other jobs in the order of the active list, which the host
+// keeps sorted by total paths (shortest job first, then arrival): capacity
+// goes to one job at a time, so a tick's paths mostly trace one scene, as one
+// job alone would, and a medium job does not wait behind a huge one.  Every
+// free slot is used as before, only the split changes.  Images do not depend
+// on the split: every sample is keyed by (job seed, pixel, sample).
 __global__ void k_plan(EngineDev E, int q) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     const uint32_t n_cont = E.cnt[q];
@@ -124,7 +125,7 @@ __global__ void k_plan(EngineDev E, int q) {
         const unsigned long long rem = J.total_samples - J.next_sample;
         if (rem * J.roles <= share) left -= uint32_t(rem) * J.roles;
     }
-    for (uint32_t a = 0; a < na; ++a) {  // those, and the rest oldest first
+    for (uint32_t a = 0; a < na; ++a) {  // those, and the rest in list order
         const uint32_t j = E.active[a];
         JobDev& J = E.jobs[j];
         const unsigned long long rem = J.total_samples - J.next_sample;
@@ -391,7 +392,8 @@ struct PathEngine {
     cudaStream_t captured_stream = nullptr;
     int parity = 0;
     uint64_t ticks = 0;
-    std::vector<uint32_t> active;
+    std::vector<uint32_t> active;   // job slots, fewest total paths first (ties: arrival order)
+    std::vector<unsigned long long> total_paths = std::vector<unsigned long long>(kMaxActiveJobs, 0);
     unsigned long long* done_h = nullptr;
     // plain renders: completion events of the two ticks in flight, and the
     // engine's counters (paths, extend rays, shadow rays) as pinned copies,
@@ -523,7 +525,11 @@ size_t engine_update(PathEngine* e, const std::vector<std::pair<uint32_t, JobDev
         AR_CUDA(cudaMemcpyAsync(e->E.jobs + slot, &st.jobs[i], sizeof(JobDev), cudaMemcpyHostToDevice,
                                 e->ctx->stream));
         e->active.push_back(slot);
+        e->total_paths[slot] = adds[i].second.total_paths;
     }
+    // the tick plan serves jobs past their equal share in this order
+    std::stable_sort(e->active.begin(), e->active.end(),
+                     [&](uint32_t a, uint32_t b) { return e->total_paths[a] < e->total_paths[b]; });
     for (size_t i = 0; i < e->active.size(); ++i) st.active[i] = e->active[i];
     st.active[kMaxActiveJobs] = uint32_t(e->active.size());
     if (!e->active.empty())

@@ -334,18 +334,20 @@ struct ServerImpl {
             std::vector<BdSegment> segs;
             // A waiting job whose remaining samples fit in an equal share of the
             // batch takes them all; the rest of the batch goes to the other jobs
-            // oldest first (as the PT tick plan does), so large jobs run one
-            // after another and a batch mostly traces one scene.
+            // shortest job first, then by arrival (as the PT tick plan does), so
+            // one job at a time fills the batch and it mostly traces one scene.
             const uint32_t cap = bdpt_batch_capacity(bdpt[lane]);
-            uint32_t waiting = 0;
-            for (SJob* j : active_bd) waiting += j->bd_issued ? 0u : 1u;
-            const uint64_t share = waiting ? cap / waiting : 0;
-            uint64_t left = cap;
+            std::vector<SJob*> order;
             for (SJob* j : active_bd)
-                if (!j->bd_issued && j->samples - j->bd_next <= share) left -= j->samples - j->bd_next;
+                if (!j->bd_issued) order.push_back(j);
+            std::stable_sort(order.begin(), order.end(),
+                             [](const SJob* a, const SJob* b) { return a->samples < b->samples; });
+            const uint64_t share = order.empty() ? 0 : cap / order.size();
+            uint64_t left = cap;
+            for (SJob* j : order)
+                if (j->samples - j->bd_next <= share) left -= j->samples - j->bd_next;
             uint32_t used = 0;
-            for (SJob* j : active_bd) {
-                if (j->bd_issued) continue;
+            for (SJob* j : order) {
                 const uint64_t rem = j->samples - j->bd_next;
                 uint64_t take = rem;
                 if (rem > share) {

@@ -687,20 +687,23 @@ __global__ void __launch_bounds__(256) k_bd_scatter(BdParams P) {
 // Copies every sample's vertices to its sorted position oi (reads scattered,
 // writes coalesced), so k_bd_connect, whose thread oi handles sample
 // order[oi], reads vertex k of 32 consecutive samples as one contiguous block.
+// One thread per (depth k, position oi), oi fastest: a warp copies depth k of
+// 32 consecutive positions, and many independent copies are in flight.
 __global__ void __launch_bounds__(256) k_bd_permute(BdParams P) {
     const uint32_t ns = P.dyn[0];
-    for (uint32_t oi = blockIdx.x * blockDim.x + threadIdx.x; oi < ns; oi += gridDim.x * blockDim.x) {
+    const uint64_t total = uint64_t(ns) * P.maxv;
+    for (uint64_t w = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; w < total;
+         w += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t k = uint32_t(w / ns), oi = uint32_t(w - uint64_t(k) * ns);
         const uint32_t si = P.order[oi];
         for (uint32_t sub = 0; sub < 2; ++sub) {
-            const uint32_t n = P.nv[sub * P.cap + si];
-            for (uint32_t k = 0; k < n; ++k) {
-                const size_t from = vidx(P, sub, k, si), to = vidx(P, sub, k, oi);
-                P.sva[to] = P.va[from];
-                P.svb[to] = P.vb[from];
-                const float4 c = P.vc[from];
-                P.svc[to] = c;
-                if ((__float_as_uint(c.w) >> 28) & 1u) P.svuv[to] = P.vuv[from];  // textured vertices only
-            }
+            if (k >= P.nv[sub * P.cap + si]) continue;
+            const size_t from = vidx(P, sub, k, si), to = vidx(P, sub, k, oi);
+            P.sva[to] = P.va[from];
+            P.svb[to] = P.vb[from];
+            const float4 c = P.vc[from];
+            P.svc[to] = c;
+            if ((__float_as_uint(c.w) >> 28) & 1u) P.svuv[to] = P.vuv[from];  // textured vertices only
         }
     }
 }

@@ -147,3 +147,30 @@ def test_graph_replay_across_streams_and_depths(ctx):
             np.testing.assert_allclose(deep.render(scene, cam, 32, 32).rgb, want_deep, rtol=1e-6, atol=1e-7)
     finally:
         ctx.set_stream(None)
+
+
+@pytest.mark.parametrize("kind", ["pt", "bdpt"])
+def test_split_order_shortest_first(ctx, kind):
+    """Past the equal share, capacity goes to the waiting jobs shortest first
+    (ties in arrival order): a medium job that does not fit in its share,
+    queued behind three large jobs, finishes before the second and third of
+    them, and the large ones finish one after another in arrival order."""
+    cb, cam = S.cornell_box(1)
+    scene = agentray.Scene(ctx, cb)
+    if kind == "pt":
+        # 2^16 path slots: each large job is 16 pool-fulls, the medium one 2
+        srv = agentray.Server(ctx, path_capacity=1 << 16)
+        large = [(_pt(16, seed=10 + k, f64=False), 256, 256) for k in range(3)]
+        medium = (_pt(8, seed=20, f64=False), 128, 128)
+    else:
+        # 2^14-sample batches: each large job is 8 batches, the medium one 2
+        srv = agentray.Server(ctx, path_capacity=1 << 16, bdpt_batch_samples=1 << 14)
+        large = [(_bdpt(8, seed=10 + k, f64=False), 128, 128) for k in range(3)]
+        medium = (_bdpt(8, seed=20, f64=False), 64, 64)
+    ids = [srv.submit(scene, cam, integ, w, h) for integ, w, h in large]
+    mid = srv.submit(scene, cam, *medium)
+    done = [srv.wait(j)["done_ms"] for j in ids]
+    m_done = srv.wait(mid)["done_ms"]
+    srv.close()
+    assert done[0] < done[1] < done[2]
+    assert m_done < done[1]

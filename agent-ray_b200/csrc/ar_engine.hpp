@@ -52,9 +52,12 @@ void engine_add_job(PathEngine* e, uint32_t slot, const JobDev& job);
 // Removes a finished job from the active list.
 void engine_remove_job(PathEngine* e, uint32_t slot);
 // Batched form of the two calls above: one staged upload for many changes.
-// Returns the bytes copied host -> device.
+// The tick plan serves jobs past their equal share in the order of the active
+// list: `order`, when given, is that list (a permutation of the active slots
+// after the changes); otherwise the slots are sorted by total paths, ties in
+// arrival order.  Returns the bytes copied host -> device.
 size_t engine_update(PathEngine* e, const std::vector<std::pair<uint32_t, JobDev>>& adds,
-                     const std::vector<uint32_t>& removes);
+                     const std::vector<uint32_t>& removes, const std::vector<uint32_t>* order = nullptr);
 // Enqueues one tick (graph replay) on the context stream.
 void engine_tick(PathEngine* e);
 // Enqueues an async copy of every job's done_paths into pinned host memory;

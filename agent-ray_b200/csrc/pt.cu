@@ -102,9 +102,10 @@ __device__ __forceinline__ void deposit(const EngineDev& E, uint32_t job, uint32
 // in an equal share of the free slots takes them all (so a small job finishes
 // in the tick it arrives instead of waiting behind a large one); what those
 // leave goes to the other jobs in the order of the active list, which the host
-// keeps sorted by total paths (shortest job first, then arrival): capacity
-// goes to one job at a time, so a tick's paths mostly trace one scene, as one
-// job alone would, and a medium job does not wait behind a huge one.  Every
+// sets (by default fewest total paths first, ties in arrival order; the
+// server ages that order by waiting time): capacity goes to one job at a time,
+// so a tick's paths mostly trace one scene, as one job alone would, and a
+// medium job does not wait behind a huge one.  Every
 // free slot is used as before, only the split changes.  Images do not depend
 // on the split: every sample is keyed by (job seed, pixel, sample).
 __global__ void k_plan(EngineDev E, int q) {
@@ -392,7 +393,7 @@ struct PathEngine {
     cudaStream_t captured_stream = nullptr;
     int parity = 0;
     uint64_t ticks = 0;
-    std::vector<uint32_t> active;   // job slots, fewest total paths first (ties: arrival order)
+    std::vector<uint32_t> active;   // job slots in the order the tick plan serves them past their share
     std::vector<unsigned long long> total_paths = std::vector<unsigned long long>(kMaxActiveJobs, 0);
     unsigned long long* done_h = nullptr;
     // plain renders: completion events of the two ticks in flight, and the
@@ -508,28 +509,43 @@ PathEngine* engine_create(ar_context* ctx, uint32_t capacity) {
 void engine_destroy(PathEngine* e) { delete e; }
 
 size_t engine_update(PathEngine* e, const std::vector<std::pair<uint32_t, JobDev>>& adds,
-                     const std::vector<uint32_t>& removes) {
-    if (adds.empty() && removes.empty()) return 0;
+                     const std::vector<uint32_t>& removes, const std::vector<uint32_t>* order) {
+    if (adds.empty() && removes.empty() && !order) return 0;
+    // the active list after the changes, checked before anything is copied
+    std::vector<uint32_t> next = e->active;
     for (uint32_t slot : removes) {
-        auto it = std::find(e->active.begin(), e->active.end(), slot);
-        if (it != e->active.end()) e->active.erase(it);
+        auto it = std::find(next.begin(), next.end(), slot);
+        if (it != next.end()) next.erase(it);
     }
-    AR_REQUIRE(e->active.size() + adds.size() <= kMaxActiveJobs, AR_ERR_REJECTED, "too many active jobs");
+    AR_REQUIRE(next.size() + adds.size() <= kMaxActiveJobs, AR_ERR_REJECTED, "too many active jobs");
+    for (const auto& a : adds) {
+        AR_REQUIRE(a.first < kMaxActiveJobs, AR_ERR_INVALID_ARGUMENT, "job slot out of range");
+        next.push_back(a.first);
+    }
+    if (order) {
+        std::vector<uint32_t> x = next, y = *order;
+        std::sort(x.begin(), x.end());
+        std::sort(y.begin(), y.end());
+        AR_REQUIRE(x == y, AR_ERR_INTERNAL, "engine order is not a permutation of the active jobs");
+    }
     auto& st = e->stage[e->stage_next];
     e->stage_next ^= 1;
     AR_CUDA(cudaEventSynchronize(st.ev));  // its previous copies have been consumed
     for (size_t i = 0; i < adds.size(); ++i) {
         const uint32_t slot = adds[i].first;
-        AR_REQUIRE(slot < kMaxActiveJobs, AR_ERR_INVALID_ARGUMENT, "job slot out of range");
         st.jobs[i] = adds[i].second;
         AR_CUDA(cudaMemcpyAsync(e->E.jobs + slot, &st.jobs[i], sizeof(JobDev), cudaMemcpyHostToDevice,
                                 e->ctx->stream));
-        e->active.push_back(slot);
         e->total_paths[slot] = adds[i].second.total_paths;
     }
     // the tick plan serves jobs past their equal share in this order
-    std::stable_sort(e->active.begin(), e->active.end(),
-                     [&](uint32_t a, uint32_t b) { return e->total_paths[a] < e->total_paths[b]; });
+    if (order) {
+        next = *order;
+    } else {
+        std::stable_sort(next.begin(), next.end(),
+                         [&](uint32_t x, uint32_t y) { return e->total_paths[x] < e->total_paths[y]; });
+    }
+    e->active.swap(next);
     for (size_t i = 0; i < e->active.size(); ++i) st.active[i] = e->active[i];
     st.active[kMaxActiveJobs] = uint32_t(e->active.size());
     if (!e->active.empty())

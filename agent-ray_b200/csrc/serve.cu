@@ -140,6 +140,29 @@ struct ServerImpl {
     std::vector<uint32_t> free_slots;
     uint64_t film_in_use = 0;
     ar_server_stats stats{};
+    // Order of the jobs past their equal share (PT ticks and BDPT batches):
+    // size / (1 + waited / kAgingMs), smallest first, ties in arrival order.
+    // Shortest job first while waits are short; a large job's key shrinks as
+    // it waits, so smaller arrivals cannot hold it back indefinitely.  The PT
+    // order is re-sent at every engine update and at most every kReorderMs.
+    static constexpr double kAgingMs = 2000.0, kReorderMs = 50.0;
+    double last_reorder_ms = 0;
+    std::vector<uint32_t> pt_order_sent;
+    double age_key(const SJob* j, uint64_t size, double now) const {
+        return double(size) / (1.0 + std::max(0.0, now - j->t_admit) / kAgingMs);
+    }
+    std::vector<uint32_t> pt_order() {
+        const double now = now_ms();
+        std::vector<SJob*> v = active_pt;
+        std::stable_sort(v.begin(), v.end(), [&](const SJob* a, const SJob* b) {
+            return age_key(a, a->total_paths, now) < age_key(b, b->total_paths, now);
+        });
+        std::vector<uint32_t> slots;
+        for (SJob* j : v) slots.push_back(j->slot);
+        last_reorder_ms = now;
+        pt_order_sent = slots;
+        return slots;
+    }
     // PT tick throttle and done snapshots
     static constexpr int kInflight = 4;
     cudaEvent_t tick_ev[kInflight] = {};
@@ -246,7 +269,10 @@ struct ServerImpl {
             j->status = AR_JOB_RUNNING;
             j->t_admit = now_ms();
         }
-        if (!adds.empty()) stats.h2d_bytes += engine_update(engine, adds, {});
+        if (!adds.empty()) {
+            const std::vector<uint32_t> order = pt_order();
+            stats.h2d_bytes += engine_update(engine, adds, {}, &order);
+        }
     }
 
     // Converts / reconstructs the film and copies it to the caller's buffer.
@@ -299,7 +325,15 @@ struct ServerImpl {
                 }
             }
             active_pt.swap(still);
-            if (!removes.empty()) stats.h2d_bytes += engine_update(engine, {}, removes);
+            if (!removes.empty()) {
+                const std::vector<uint32_t> order = pt_order();
+                stats.h2d_bytes += engine_update(engine, {}, removes, &order);
+            }
+        }
+        if (active_pt.size() > 1 && now_ms() - last_reorder_ms >= kReorderMs) {
+            const std::vector<uint32_t> before = pt_order_sent;
+            const std::vector<uint32_t> order = pt_order();
+            if (order != before) stats.h2d_bytes += engine_update(engine, {}, {}, &order);
         }
         if (!snap_pending) {
             engine_snapshot_done(engine);
@@ -334,14 +368,16 @@ struct ServerImpl {
             std::vector<BdSegment> segs;
             // A waiting job whose remaining samples fit in an equal share of the
             // batch takes them all; the rest of the batch goes to the other jobs
-            // shortest job first, then by arrival (as the PT tick plan does), so
-            // one job at a time fills the batch and it mostly traces one scene.
+            // in the aged shortest-first order (as the PT tick plan does), so one
+            // job at a time fills the batch and it mostly traces one scene.
             const uint32_t cap = bdpt_batch_capacity(bdpt[lane]);
             std::vector<SJob*> order;
             for (SJob* j : active_bd)
                 if (!j->bd_issued) order.push_back(j);
-            std::stable_sort(order.begin(), order.end(),
-                             [](const SJob* a, const SJob* b) { return a->samples < b->samples; });
+            const double now = now_ms();
+            std::stable_sort(order.begin(), order.end(), [&](const SJob* a, const SJob* b) {
+                return age_key(a, a->samples, now) < age_key(b, b->samples, now);
+            });
             const uint64_t share = order.empty() ? 0 : cap / order.size();
             uint64_t left = cap;
             for (SJob* j : order)
@@ -486,6 +522,19 @@ struct ServerImpl {
                 maybe_dump();
             } catch (const ArError& e) {
                 set_error(e.msg);
+                // Drop the failed PT jobs from the engine's active list too, so
+                // that later admissions start from a list that matches
+                // active_pt.  Their slots stay out of the free list: paths of a
+                // failed job may still be in flight, keyed by its slot.
+                std::vector<uint32_t> slots;
+                for (SJob* j : active_pt)
+                    if (j->slot != kInvalid) slots.push_back(j->slot);
+                try {
+                    if (!slots.empty()) engine_update(engine, {}, slots);
+                } catch (const ArError&) {
+                    // the engine could not be updated (a sticky CUDA error)
+                }
+                pt_order_sent.clear();
                 for (SJob* j : active_pt) fail(j, e.code);
                 for (SJob* j : active_bd) fail(j, e.code);
                 for (SJob* j : finishing) fail(j, e.code);

@@ -375,8 +375,12 @@ int ar_poisson_sor_static(const ar_integrator_cfg* cfg, uint32_t width, uint32_t
  * into shared wavefront kernels: PT and GDPT paths stream through one path pool
  * refilled every tick; BDPT jobs share sample batches.  Jobs are admitted in
  * arrival order while their films fit the HBM budget; a job whose films alone
- * exceed the budget is REJECTED.  Results are written to the caller's host
- * buffer (W*H*3 f32, like ar_render) before the job reports DONE. */
+ * exceed the budget is REJECTED.  Each tick (and each BDPT batch), a running
+ * job whose remaining samples fit in an equal share of the free capacity takes
+ * them all; the rest goes to the other jobs smallest first, a job's size
+ * discounted by 1 + (seconds waited) / 2, ties in arrival order.  Results are
+ * written to the caller's host buffer (W*H*3 f32, like ar_render) before the
+ * job reports DONE. */
 typedef struct ar_server ar_server;
 
 enum ar_job_status {
